@@ -1,0 +1,159 @@
+"""Pin the oracle: the C restatement (oracle/oracle.c) against grids written by
+the hpcscan reference itself (tests/golden/, made by make_golden.py from the
+reference CPU binaries built unchanged).
+
+FP32 and FP64 elementwise results (fill, FD_D2, Laplacian, one propagator
+step) are compared BIT-EXACTLY; the reference's printed L1 errors and
+errTestCase are compared to the 6 significant digits it prints.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from hpcscan_b200 import layout as L
+from hpcscan_b200.propa_setup import eigen_setup
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+MANIFEST = json.load(open(os.path.join(GOLDEN, "manifest.json")))
+
+DEFAULT_PARAMS = (0.8, 0.9, 1.0, 1.1)   # src/config.cpp:72-75
+
+
+def flag_value(flags, name, default):
+    return float(flags[flags.index(name) + 1]) if name in flags else default
+
+
+def pad_kwargs(flags):
+    import re
+    kw = {"auto_pad": "-autoPad" in flags, "add_pad": [None] * 3, "mul_pad": [None] * 3}
+    for i, f in enumerate(flags):
+        m = re.match(r"-n([123])(Add|Mul)Pad", f)
+        if m:
+            kw["add_pad" if m.group(2) == "Add" else "mul_pad"][int(m.group(1)) - 1] = int(flags[i + 1])
+    kw["add_pad"], kw["mul_pad"] = tuple(kw["add_pad"]), tuple(kw["mul_pad"])
+    return kw
+
+
+def fd_input(oracle, meta):
+    """The FD_D2 test input U = a4 sin(a1 x1) sin(a2 x2) sin(a3 x3) on ALL_POINTS
+    (src/testCase_FD_D2.cpp:65-74)."""
+    flags = meta["flags"]
+    lay = L.reference_layout(meta["dim"], *meta["n"], order=meta["order"], prec=meta["prec"],
+                             **pad_kwargs(flags))
+    p = [flag_value(flags, f"-param{i + 1}", DEFAULT_PARAMS[i]) for i in range(4)]
+    a = [L.PI * p[0], L.PI * p[1], L.PI * p[2]]
+    samp = L.unit_sampling(lay)
+    tabs = L.fill_tables(lay, samp, L.ALL_POINTS, (L.FUNC_SINE,) * 3, a)
+    u = oracle.alloc(lay)
+    oracle.fill_sep(lay, u, lay.box(L.ALL_POINTS), tabs, p[3])
+    return lay, samp, u, a, p
+
+
+FD_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "FD_D2")
+PROPA_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "Propa")
+
+
+@pytest.mark.parametrize("fixture", FD_FIXTURES)
+def test_fd_d2_matches_reference(oracle, fixture):
+    meta = MANIFEST[fixture]
+    gold = np.load(os.path.join(GOLDEN, fixture))
+    lay, samp, u, a, p = fd_input(oracle, meta)
+    if "U" in gold:
+        # the separable fill is bit-identical (FP64 tables, product cast to Myfloat)
+        assert np.array_equal(u, gold["U"])
+    inv2 = L.inv2_spacing(samp, lay.prec)
+    for case in meta["cases"]:
+        w = oracle.alloc(lay)
+        if case.startswith("Axis"):
+            oracle.fd_d2(lay, int(case[-1]), u, w, inv2)
+        else:
+            oracle.laplacian(lay, u, w, inv2)
+        got = lay.inner(w)
+        assert np.array_equal(got, gold[case]), (case, np.abs(got - gold[case]).max())
+
+
+@pytest.mark.parametrize("fixture", [f for f in FD_FIXTURES if "all" not in f])
+def test_fd_d2_l1_error_matches_reference(oracle, fixture):
+    """The analytic-reference L1 error the reference printed (Test PASSED / L1 err.)."""
+    meta = MANIFEST[fixture]
+    lay, samp, u, a, p = fd_input(oracle, meta)
+    inv2 = L.inv2_spacing(samp, lay.prec)
+    tabs = L.fill_tables(lay, samp, L.ALL_POINTS, (L.FUNC_SINE,) * 3, a)
+    errs = []
+    for case in meta["cases"]:
+        w = oracle.alloc(lay)
+        r = oracle.alloc(lay)
+        if case.startswith("Axis"):
+            ax = int(case[-1])
+            oracle.fd_d2(lay, ax, u, w, inv2)
+            amp = -a[ax - 1] * a[ax - 1] * p[3]
+        else:
+            oracle.laplacian(lay, u, w, inv2)
+            amp = -sum(a[i] * a[i] for i in range(lay.dim)) * p[3] if lay.dim > 1 else \
+                -a[0] * a[0] * p[3]
+            if lay.dim == 2:
+                amp = -(a[0] * a[0] + a[1] * a[1]) * p[3]
+            elif lay.dim == 3:
+                amp = -(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]) * p[3]
+        oracle.fill_sep(lay, r, lay.box(L.ALL_POINTS), tabs, amp)
+        err = oracle.l1_err(lay, w, r, lay.box(L.INNER_POINTS))
+        errs.append(float(np.float32(err)) if lay.prec == "f32" else err)
+    ref = meta["l1_err"]
+    assert len(errs) == len(ref)
+    np.testing.assert_allclose(errs, ref, rtol=2e-5)
+
+
+@pytest.mark.parametrize("fixture", PROPA_FIXTURES)
+def test_propa_matches_reference(oracle, fixture):
+    meta = MANIFEST[fixture]
+    gold = np.load(os.path.join(GOLDEN, fixture))
+    flags = meta["flags"]
+    lay = L.reference_layout(meta["dim"], *meta["n"], order=meta["order"], prec=meta["prec"])
+    setup = eigen_setup(lay, ratio_cfl=flag_value(flags, "-ratioCFL", 1.0),
+                        nt=int(flag_value(flags, "-nt", 20)),
+                        snap_inc=int(flag_value(flags, "-snapInc", 1)),
+                        modes=tuple(flag_value(flags, f"-param{i + 1}", DEFAULT_PARAMS[i])
+                                    for i in range(3)))
+    assert setup.nt == meta["nt"]
+    assert abs(setup.dt - meta["dt"]) <= 1e-5 * meta["dt"]
+    checks = []
+
+    def on_check(it, prn, ref):
+        checks.append(np.array(lay.inner(prn)))
+
+    _, _, err = oracle.propagate(lay, setup, split=meta["propagator"] == "Ac2SplitComp",
+                                 on_check=on_check)
+    assert len(checks) == len([k for k in gold.files if k.startswith("prn_")])
+    for i, got in enumerate(checks):
+        assert np.array_equal(got, gold[f"prn_{i}"]), (i, np.abs(got - gold[f"prn_{i}"]).max())
+    assert abs(err - meta["err_test_case"]) <= 2e-5 * abs(meta["err_test_case"])
+
+
+def test_coefficient_sums_vanish():
+    """testCase_Util known answer: sum of FD_D2 coefficients = 0 (src/testCase_Util.cpp:602-619)."""
+    from hpcscan_b200 import fdm
+    for o in fdm.ORDERS:
+        assert abs(fdm.sum_coef(o, np.float64)) < 1e-12
+        assert abs(fdm.sum_coef(o, np.float32)) < 1e-6
+
+
+def test_layouts_match_reference_rules():
+    """Full dimensions of the reference layout for the fixtures' flags equal
+    what the reference wrote in its .grid.info files (checked at fixture time);
+    spot-check the rules directly."""
+    lay = L.reference_layout(3, 200, 200, 200, order=8)
+    assert (lay.n1, lay.n2, lay.n3) == (208, 208, 208)
+    lay = L.reference_layout(3, 21, 20, 20, order=6, auto_pad=True)   # odd halo: offset 1 in FP32
+    assert lay.a1.inner_start == 4 and lay.n1 % 2 == 0
+    lay = L.reference_layout(3, 21, 20, 20, order=6, prec="f64")
+    assert lay.a1.inner_start == 3
+    b = L.b200_layout(3, 512, 512, 512, order=8)
+    assert b.a1.inner_start % 4 == 0 and (b.n1 * 4) % 32 == 0
+    for o in (2, 4, 6, 8, 10, 12, 14, 16):
+        for prec, al in (("f32", 4), ("f64", 2), ("f16", 8), ("bf16", 8)):
+            b = L.b200_layout(3, 33, 20, 21, order=o, prec=prec)
+            assert b.a1.inner_start % al == 0
+            assert (b.n1 * b.elem_size) % 32 == 0
+            assert b.a1.halo2_end < b.n1
