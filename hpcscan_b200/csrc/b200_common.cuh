@@ -1,0 +1,184 @@
+// Shared device/host helpers of the hpcscan_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hpcscan_b200.h"
+
+namespace b200 {
+
+// ---- error reporting (b200_runtime.cu) -------------------------------------------------------
+int set_error(int code, const char* fmt, ...);
+int cuda_error(cudaError_t err, const char* what);
+// After a kernel launch: report a launch-configuration error without synchronising.
+int check_launch(const char* what);
+
+// ---- per-device scratch (b200_runtime.cu) ----------------------------------------------------
+// A device buffer of at least `bytes`, owned by the library for the current device and reused
+// by every call (calls on one device are serialised by the caller's stream discipline).
+int scratch(size_t bytes, void** ptr);
+// Pinned host staging of at least `bytes` for small results.
+int host_staging(size_t bytes, void** ptr);
+int num_sms();
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---- argument validation -----------------------------------------------------------------------
+int check_layout(const b200_layout* lay);
+int check_box(const b200_layout* lay, const b200_box* box);
+int check_order(int order);
+int check_field(const b200_field& f, const char* name);
+inline int64_t npoint(const b200_layout* lay) { return lay->n1 * lay->n2 * lay->n3; }
+
+// ---- storage traits ----------------------------------------------------------------------------
+// S = storage type, C = compute type (Myfloat / Myfloat2 of the reference builds).
+template <typename S> struct Storage;
+template <> struct Storage<float> {
+	using C = float;
+	static __device__ __forceinline__ float load(float v) { return v; }
+	static __device__ __forceinline__ float store(float v) { return v; }
+	static __device__ __forceinline__ float store_d(double v) { return __double2float_rn(v); }
+};
+template <> struct Storage<double> {
+	using C = double;
+	static __device__ __forceinline__ double load(double v) { return v; }
+	static __device__ __forceinline__ double store(double v) { return v; }
+	static __device__ __forceinline__ double store_d(double v) { return v; }
+};
+template <> struct Storage<__half> {
+	using C = float;
+	static __device__ __forceinline__ float load(__half v) { return __half2float(v); }
+	static __device__ __forceinline__ __half store(float v) { return __float2half_rn(v); }
+	static __device__ __forceinline__ __half store_d(double v) { return __double2half(v); }
+};
+template <> struct Storage<__nv_bfloat16> {
+	using C = float;
+	static __device__ __forceinline__ float load(__nv_bfloat16 v) { return __bfloat162float(v); }
+	static __device__ __forceinline__ __nv_bfloat16 store(float v) { return __float2bfloat16_rn(v); }
+	static __device__ __forceinline__ __nv_bfloat16 store_d(double v) { return __double2bfloat16(v); }
+};
+
+// ---- arithmetic with explicit rounding ---------------------------------------------------------
+// EXACT = true: every multiply and add is a separately rounded IEEE operation (no FMA
+// contraction), the order of the reference's CPU expressions compiled without FP
+// contraction; the results are then bit-identical to the reference CPU path.
+template <bool EXACT> struct Arith;
+template <> struct Arith<true> {
+	static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+	static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+	static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+	static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+	static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+	static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+};
+template <> struct Arith<false> {
+	template <typename C> static __device__ __forceinline__ C mul(C a, C b) { return a * b; }
+	template <typename C> static __device__ __forceinline__ C add(C a, C b) { return a + b; }
+	template <typename C> static __device__ __forceinline__ C sub(C a, C b) { return a - b; }
+};
+
+// ---- FD_D2 coefficients (reference src/fdm.h:277-545), exact rationals --------------------------
+// Stored in FP64; the compute type rounds them exactly as the reference's `const Myfloat2`.
+struct D2Table {
+	double c[9][9];
+};
+__host__ __device__ constexpr D2Table make_d2_table()
+{
+	return D2Table{{
+		{0, 0, 0, 0, 0, 0, 0, 0, 0},
+		{-2.0, 1.0, 0, 0, 0, 0, 0, 0, 0},
+		{-5. / 2., 4. / 3., -1. / 12., 0, 0, 0, 0, 0, 0},
+		{-49. / 18., 3. / 2., -3. / 20., 1. / 90., 0, 0, 0, 0, 0},
+		{-205. / 72., 8. / 5., -1 / 5., 8. / 315., -1 / 560., 0, 0, 0, 0},
+		{-5269. / 1800., 5. / 3., -5. / 21., 5. / 126., -5. / 1008., 1. / 3150., 0, 0, 0},
+		{-5369. / 1800., 12. / 7., -15. / 56., 10. / 189., -1. / 112., 2. / 1925., -1. / 16632., 0, 0},
+		{-266681. / 88200., 7. / 4., -7. / 24., 7. / 108., -7. / 528., 7. / 3300., -7. / 30888.,
+		 1. / 84084., 0},
+		{-1077749. / 352800., 16. / 9., -14. / 45., 112. / 1485., -7. / 396., 112. / 32175.,
+		 -2. / 3861., 16. / 315315., -1. / 411840.},
+	}};
+}
+
+template <typename C, int R, int K>
+__device__ __forceinline__ C d2c()
+{
+	constexpr D2Table t = make_d2_table();
+	return static_cast<C>(t.c[R][K]);
+}
+
+// Second derivative from values v(k), k = -R..R, around a point, with the reference's
+// association: ((A0 u + A1 (u+1 + u-1)) + A2 (u+2 + u-2)) + ... then * inv2.
+// O2 is written (A0 u + u+1) + u-1 with no A1 (src/fdm.h:286-296).
+template <typename C, int R, bool EXACT, typename F>
+__device__ __forceinline__ C d2_axis(F v, C inv2)
+{
+	using A = Arith<EXACT>;
+	C acc = A::mul(d2c<C, R, 0>(), v(0));
+	if constexpr (R == 1) {
+		return A::mul(A::add(A::add(acc, v(1)), v(-1)), inv2);
+	} else {
+		acc = A::add(acc, A::mul(d2c<C, R, 1>(), A::add(v(1), v(-1))));
+		acc = A::add(acc, A::mul(d2c<C, R, 2>(), A::add(v(2), v(-2))));
+		if constexpr (R >= 3) acc = A::add(acc, A::mul(d2c<C, R, 3>(), A::add(v(3), v(-3))));
+		if constexpr (R >= 4) acc = A::add(acc, A::mul(d2c<C, R, 4>(), A::add(v(4), v(-4))));
+		if constexpr (R >= 5) acc = A::add(acc, A::mul(d2c<C, R, 5>(), A::add(v(5), v(-5))));
+		if constexpr (R >= 6) acc = A::add(acc, A::mul(d2c<C, R, 6>(), A::add(v(6), v(-6))));
+		if constexpr (R >= 7) acc = A::add(acc, A::mul(d2c<C, R, 7>(), A::add(v(7), v(-7))));
+		if constexpr (R >= 8) acc = A::add(acc, A::mul(d2c<C, R, 8>(), A::add(v(8), v(-8))));
+		return A::mul(acc, inv2);
+	}
+}
+
+// Leapfrog update of computePressureWithFD: (2 prc - prn) + coef * lap.
+template <typename C, bool EXACT>
+__device__ __forceinline__ C leapfrog(C prc, C prn, C coef, C lap)
+{
+	using A = Arith<EXACT>;
+	return A::add(A::sub(A::mul(static_cast<C>(2.0), prc), prn), A::mul(coef, lap));
+}
+
+// Dispatch a runtime FD order to a compile-time half width R.
+template <typename F>
+int dispatch_order(int order, F&& f)
+{
+	switch (order) {
+	case 2: return f(std::integral_constant<int, 1>{});
+	case 4: return f(std::integral_constant<int, 2>{});
+	case 6: return f(std::integral_constant<int, 3>{});
+	case 8: return f(std::integral_constant<int, 4>{});
+	case 10: return f(std::integral_constant<int, 5>{});
+	case 12: return f(std::integral_constant<int, 6>{});
+	case 14: return f(std::integral_constant<int, 7>{});
+	case 16: return f(std::integral_constant<int, 8>{});
+	default: return set_error(B200_ERR_ARG, "FD order %d not supported (2..16, even)", order);
+	}
+}
+
+// Dispatch a storage dtype code to a C++ type.
+template <typename F>
+int dispatch_dtype(int dtype, F&& f)
+{
+	switch (dtype) {
+	case B200_F32: return f(float{});
+	case B200_F64: return f(double{});
+	case B200_F16: return f(__half{});
+	case B200_BF16: return f(__nv_bfloat16{});
+	default: return set_error(B200_ERR_ARG, "unknown dtype %d", dtype);
+	}
+}
+
+inline int dtype_size(int dtype)
+{
+	switch (dtype) {
+	case B200_F32: return 4;
+	case B200_F64: return 8;
+	case B200_F16: return 2;
+	case B200_BF16: return 2;
+	default: return 0;
+	}
+}
+
+}  // namespace b200

@@ -1,0 +1,605 @@
+// Grid operations of the hpcscan_b200 C ABI other than the stencils: fills, the
+// anti-mirror boundary condition, the split pressure update and the FP64 norms.
+#include "b200_common.cuh"
+
+namespace b200 {
+
+namespace {
+
+constexpr int kRowThreads = 256;
+
+struct Box3 {
+	int64_t i1s, i2s, i3s;
+	int nx, ny, nz;
+};
+
+Box3 to_box3(const b200_box* b)
+{
+	return Box3{b->i1s, b->i2s, b->i3s, (int)(b->i1e - b->i1s + 1), (int)(b->i2e - b->i2s + 1),
+			(int)(b->i3e - b->i3s + 1)};
+}
+
+dim3 row_grid(const Box3& b)
+{
+	// blocks: x over i1 chunks, y over i2, z over i3 (grid.y/z limit 65535 — grids here are far
+	// smaller per axis)
+	return dim3((unsigned)((b.nx + kRowThreads - 1) / kRowThreads), (unsigned)b.ny, (unsigned)b.nz);
+}
+
+// ---- fills ------------------------------------------------------------------------------------
+template <typename S>
+__global__ void k_fill_const(S* __restrict__ u, int64_t n1, int64_t n12, Box3 b, S val)
+{
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	if (x >= b.nx) return;
+	const int64_t i1 = b.i1s + x, i2 = b.i2s + blockIdx.y, i3 = b.i3s + blockIdx.z;
+	u[i1 + i2 * n1 + i3 * n12] = val;
+}
+
+template <typename S>
+__global__ void k_fill_separable(S* __restrict__ u, int64_t n1, int64_t n12, Box3 b,
+		const double* __restrict__ v1, const double* __restrict__ v2,
+		const double* __restrict__ v3, double amp)
+{
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	if (x >= b.nx) return;
+	const int y = blockIdx.y, z = blockIdx.z;
+	// (((amp * v1) * v2) * v3), each product rounded in FP64, then one rounding to S
+	const double v = __dmul_rn(__dmul_rn(__dmul_rn(amp, v1[x]), v2[y]), v3[z]);
+	u[(b.i1s + x) + (b.i2s + y) * n1 + (b.i3s + z) * n12] = Storage<S>::store_d(v);
+}
+
+// ---- boundary condition ----------------------------------------------------------------------
+struct BcArgs {
+	int64_t n1, n12;
+	int64_t s[3], e[3];
+	int halo, dim, faces;
+};
+
+// Phase A: every halo value of the active faces, computed from the values before the
+// boundary condition. A mirror point that an earlier face (in the reference's order
+// I1HALO1, I1HALO2, I2HALO1, I2HALO2, I3HALO1, I3HALO2) sets to zero reads as zero.
+// Reads touch inner points only and writes touch halo points only, so one launch is safe.
+// Valid when every used axis has at least halo + 2 inner points (checked by the caller).
+template <typename S>
+__global__ void k_bc_halos(S* __restrict__ u, BcArgs a)
+{
+	const int axis = blockIdx.y;            // face pair along this axis
+	if (axis >= a.dim) return;
+	const int64_t nx = a.e[0] - a.s[0] + 1, ny = a.e[1] - a.s[1] + 1, nz = a.e[2] - a.s[2] + 1;
+	const int R = a.halo;
+	// positions enumerated: (side, k, other axes) with the fastest index along i1 when possible
+	int64_t count;
+	if (axis == 0) count = 2 * (int64_t)R * ny * nz;
+	else if (axis == 1) count = 2 * (int64_t)R * nx * nz;
+	else count = 2 * (int64_t)R * nx * ny;
+	const bool lo_x = a.faces & 1, hi_x = a.faces & 2, lo_y = a.faces & 4, hi_y = a.faces & 8;
+	for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+			t += (int64_t)gridDim.x * blockDim.x) {
+		int64_t i1, i2, i3, m1, m2, m3;
+		bool zero = false;
+		if (axis == 0) {
+			const int k = (int)(t % R) + 1;
+			int64_t r = t / R;
+			const int side = (int)(r % 2);
+			r /= 2;
+			if (!(a.faces & (1 << side))) continue;
+			i2 = a.s[1] + r % ny;
+			i3 = a.s[2] + r / ny;
+			i1 = side ? a.e[0] + k : a.s[0] - k;
+			m1 = side ? a.e[0] - k : a.s[0] + k;
+			m2 = i2;
+			m3 = i3;
+		} else if (axis == 1) {
+			const int64_t x = t % nx;
+			int64_t r = t / nx;
+			const int k = (int)(r % R) + 1;
+			r /= R;
+			const int side = (int)(r % 2);
+			r /= 2;
+			if (!(a.faces & (4 << side))) continue;
+			i1 = a.s[0] + x;
+			i3 = a.s[2] + r;
+			i2 = side ? a.e[1] + k : a.s[1] - k;
+			m1 = i1;
+			m2 = side ? a.e[1] - k : a.s[1] + k;
+			m3 = i3;
+			zero = (lo_x && m1 == a.s[0]) || (hi_x && m1 == a.e[0]);
+		} else {
+			const int64_t x = t % nx;
+			int64_t r = t / nx;
+			const int64_t y = r % ny;
+			r /= ny;
+			const int k = (int)(r % R) + 1;
+			r /= R;
+			const int side = (int)r;
+			if (!(a.faces & (16 << side))) continue;
+			i1 = a.s[0] + x;
+			i2 = a.s[1] + y;
+			i3 = side ? a.e[2] + k : a.s[2] - k;
+			m1 = i1;
+			m2 = i2;
+			m3 = side ? a.e[2] - k : a.s[2] + k;
+			zero = (lo_x && m1 == a.s[0]) || (hi_x && m1 == a.e[0]) || (lo_y && m2 == a.s[1]) ||
+			       (hi_y && m2 == a.e[1]);
+		}
+		const S mv = zero ? S(0.0f) : u[m1 + m2 * a.n1 + m3 * a.n12];
+		u[i1 + i2 * a.n1 + i3 * a.n12] = Storage<S>::store(-Storage<S>::load(mv));
+	}
+}
+
+// Phase B: the boundary planes (first/last inner point of each active face) set to zero.
+template <typename S>
+__global__ void k_bc_planes(S* __restrict__ u, BcArgs a)
+{
+	const int axis = blockIdx.y;
+	if (axis >= a.dim) return;
+	const int64_t nx = a.e[0] - a.s[0] + 1, ny = a.e[1] - a.s[1] + 1, nz = a.e[2] - a.s[2] + 1;
+	int64_t count = (axis == 0) ? 2 * ny * nz : (axis == 1) ? 2 * nx * nz : 2 * nx * ny;
+	for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+			t += (int64_t)gridDim.x * blockDim.x) {
+		int64_t i1, i2, i3;
+		if (axis == 0) {
+			const int side = (int)(t % 2);
+			const int64_t r = t / 2;
+			if (!(a.faces & (1 << side))) continue;
+			i1 = side ? a.e[0] : a.s[0];
+			i2 = a.s[1] + r % ny;
+			i3 = a.s[2] + r / ny;
+		} else if (axis == 1) {
+			const int64_t x = t % nx;
+			const int64_t r = t / nx;
+			const int side = (int)(r % 2);
+			if (!(a.faces & (4 << side))) continue;
+			i1 = a.s[0] + x;
+			i2 = side ? a.e[1] : a.s[1];
+			i3 = a.s[2] + r / 2;
+		} else {
+			const int64_t x = t % nx;
+			const int64_t r = t / nx;
+			const int64_t y = r % ny;
+			const int side = (int)(r / ny);
+			if (!(a.faces & (16 << side))) continue;
+			i1 = a.s[0] + x;
+			i2 = a.s[1] + y;
+			i3 = side ? a.e[2] : a.s[2];
+		}
+		u[i1 + i2 * a.n1 + i3 * a.n12] = S(0.0f);
+	}
+}
+
+// Sequential form for tiny grids (an axis with fewer than halo + 2 inner points): one face
+// per launch in the reference order, each thread owning one line normal to the face.
+template <typename S>
+__global__ void k_bc_face(S* __restrict__ u, BcArgs a, int face)
+{
+	const int axis = face / 2, side = face % 2;
+	const int64_t nx = a.e[0] - a.s[0] + 1, ny = a.e[1] - a.s[1] + 1, nz = a.e[2] - a.s[2] + 1;
+	const int64_t lines = (axis == 0) ? ny * nz : (axis == 1) ? nx * nz : nx * ny;
+	const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (t >= lines) return;
+	int64_t base, st, b;
+	if (axis == 0) {
+		base = (a.s[1] + t % ny) * a.n1 + (a.s[2] + t / ny) * a.n12;
+		st = 1;
+		b = side ? a.e[0] : a.s[0];
+	} else if (axis == 1) {
+		base = (a.s[0] + t % nx) + (a.s[2] + t / nx) * a.n12;
+		st = a.n1;
+		b = side ? a.e[1] : a.s[1];
+	} else {
+		base = (a.s[0] + t % nx) + (a.s[1] + t / nx) * a.n1;
+		st = a.n12;
+		b = side ? a.e[2] : a.s[2];
+	}
+	u[base + b * st] = S(0.0f);
+	for (int k = 1; k <= a.halo; k++) {
+		const int64_t h = side ? b + k : b - k, m = side ? b - k : b + k;
+		u[base + h * st] = Storage<S>::store(-Storage<S>::load(u[base + m * st]));
+	}
+}
+
+// ---- split update ------------------------------------------------------------------------------
+template <typename S, bool EXACT>
+__global__ void k_update_pressure(S* __restrict__ prn, const S* __restrict__ prc,
+		const S* __restrict__ coef, const S* __restrict__ lapla, int64_t n1, int64_t n12, Box3 b,
+		float coef_scale)
+{
+	using C = typename Storage<S>::C;
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	if (x >= b.nx) return;
+	const int64_t ii = (b.i1s + x) + (b.i2s + blockIdx.y) * n1 + (b.i3s + blockIdx.z) * n12;
+	C c = Storage<S>::load(coef[ii]);
+	if (coef_scale != 1.0f) c = c * (C)coef_scale;
+	prn[ii] = Storage<S>::store(leapfrog<C, EXACT>(Storage<S>::load(prc[ii]),
+			Storage<S>::load(prn[ii]), c, Storage<S>::load(lapla[ii])));
+}
+
+// ---- reductions -------------------------------------------------------------------------------
+enum RedOp { RED_SUM_ABS = 0, RED_L1 = 1, RED_MAX_ERR = 2, RED_MIN_MAX = 3, RED_L1_SEP = 4 };
+
+constexpr int kRedThreads = 256;
+
+struct RedArgs {
+	int64_t n1, n12;
+	Box3 b;
+	double s1, s2;                  // field scales
+	double max_err_float;
+	const double* v1;               // separable reference tables (RED_L1_SEP)
+	const double* v2;
+	const double* v3;
+	double amp;
+	int ref_dtype;
+};
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+__device__ __forceinline__ double warp_max(double v)
+{
+	for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+	return v;
+}
+__device__ __forceinline__ double warp_min(double v)
+{
+	for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+	return v;
+}
+
+// combine two accumulators (a: first result, b: second) over the block
+template <int OP>
+__device__ void block_combine(double& a, double& b)
+{
+	__shared__ double sa[kRedThreads / 32], sb[kRedThreads / 32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	if (OP == RED_MAX_ERR) {
+		a = warp_max(a);
+	} else if (OP == RED_MIN_MAX) {
+		a = warp_min(a);
+		b = warp_max(b);
+	} else {
+		a = warp_sum(a);
+		b = warp_sum(b);
+	}
+	if (lane == 0) {
+		sa[w] = a;
+		sb[w] = b;
+	}
+	__syncthreads();
+	if (w == 0) {
+		a = lane < kRedThreads / 32 ? sa[lane] : (OP == RED_MAX_ERR ? -1.0e308 : (OP == RED_MIN_MAX ? 1.0e308 : 0.0));
+		b = lane < kRedThreads / 32 ? sb[lane] : (OP == RED_MIN_MAX ? -1.0e308 : 0.0);
+		if (OP == RED_MAX_ERR) {
+			a = warp_max(a);
+		} else if (OP == RED_MIN_MAX) {
+			a = warp_min(a);
+			b = warp_max(b);
+		} else {
+			a = warp_sum(a);
+			b = warp_sum(b);
+		}
+	}
+}
+
+template <typename S>
+__device__ __forceinline__ double ref_value(const RedArgs& r, int x, int y, int z)
+{
+	const double v = __dmul_rn(__dmul_rn(__dmul_rn(r.amp, r.v1[x]), r.v2[y]), r.v3[z]);
+	switch (r.ref_dtype) {
+	case B200_F32: return (double)__double2float_rn(v);
+	case B200_F16: return (double)__half2float(__double2half(v));
+	case B200_BF16: return (double)__bfloat162float(__double2bfloat16(v));
+	default: return v;
+	}
+}
+
+// Stage 1: one partial (pair) per block; blocks stride over the rows (i2, i3) of the box,
+// threads along i1, so every read is coalesced. Deterministic for a given grid size.
+template <typename S, int OP>
+__global__ void __launch_bounds__(kRedThreads) k_reduce(const S* __restrict__ u1,
+		const S* __restrict__ u2, RedArgs r, double2* __restrict__ partial)
+{
+	double a = (OP == RED_MAX_ERR) ? -(double)3.402823466e+38f : (OP == RED_MIN_MAX ? 1.0e308 : 0.0);
+	double b = (OP == RED_MIN_MAX) ? -1.0e308 : 0.0;
+	const int64_t rows = (int64_t)r.b.ny * r.b.nz;
+	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+		const int y = (int)(row % r.b.ny), z = (int)(row / r.b.ny);
+		const int64_t base = r.b.i1s + (r.b.i2s + y) * r.n1 + (r.b.i3s + z) * r.n12;
+		for (int x = threadIdx.x; x < r.b.nx; x += blockDim.x) {
+			const double v1 = (double)Storage<S>::load(u1[base + x]) * r.s1;
+			if (OP == RED_SUM_ABS) {
+				a += fabs(v1);
+			} else if (OP == RED_MIN_MAX) {
+				a = fmin(a, v1);
+				b = fmax(b, v1);
+			} else {
+				double v2;
+				if (OP == RED_L1_SEP) v2 = ref_value<S>(r, x, y, z);
+				else v2 = (double)Storage<S>::load(u2[base + x]) * r.s2;
+				if (OP == RED_L1 || OP == RED_L1_SEP) {
+					a += fabs(v1 - v2);
+					b += fabs(v2);
+				} else {   // RED_MAX_ERR (src/grid.cpp:2031-2043)
+					double e;
+					if (fabsf((float)v2) < (float)r.max_err_float) e = fabs(v1 - v2);
+					else e = fabs(v1 - v2) / fabs(v2);
+					a = fmax(a, e);
+				}
+			}
+		}
+	}
+	block_combine<OP>(a, b);
+	if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(a, b);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(kRedThreads) k_reduce_final(const double2* __restrict__ partial,
+		int n, double2* __restrict__ out)
+{
+	double a = (OP == RED_MAX_ERR) ? -(double)3.402823466e+38f : (OP == RED_MIN_MAX ? 1.0e308 : 0.0);
+	double b = (OP == RED_MIN_MAX) ? -1.0e308 : 0.0;
+	for (int i = threadIdx.x; i < n; i += blockDim.x) {
+		const double2 p = partial[i];
+		if (OP == RED_MAX_ERR) {
+			a = fmax(a, p.x);
+		} else if (OP == RED_MIN_MAX) {
+			a = fmin(a, p.x);
+			b = fmax(b, p.y);
+		} else {
+			a += p.x;
+			b += p.y;
+		}
+	}
+	block_combine<OP>(a, b);
+	if (threadIdx.x == 0) *out = make_double2(a, b);
+}
+
+template <int OP>
+int run_reduce(const b200_layout* lay, const b200_field& u1, const b200_field* u2,
+		const b200_box* box, RedArgs r, double* out_a, double* out_b, void* stream)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_box(lay, box)) return rc;
+	if (int rc = check_field(u1, "u1")) return rc;
+	if (u2) {
+		if (int rc = check_field(*u2, "u2")) return rc;
+		if (u2->dtype != u1.dtype)
+			return set_error(B200_ERR_UNSUPPORTED, "norm of two grids of different storage types");
+	}
+	r.n1 = lay->n1;
+	r.n12 = lay->n1 * lay->n2;
+	r.b = to_box3(box);
+	r.s1 = u1.scale;
+	r.s2 = u2 ? u2->scale : 1.0;
+	const int64_t rows = (int64_t)r.b.ny * r.b.nz;
+	int blocks = num_sms() * 8;
+	if (rows < blocks) blocks = (int)(rows > 0 ? rows : 1);
+	void* scr;
+	if (int rc = scratch(sizeof(double2) * (blocks + 1), &scr)) return rc;
+	double2* partial = reinterpret_cast<double2*>(scr);
+	double2* result = partial + blocks;
+	cudaStream_t s = as_stream(stream);
+	int rc = dispatch_dtype(u1.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		k_reduce<S, OP><<<blocks, kRedThreads, 0, s>>>(static_cast<const S*>(u1.data),
+				u2 ? static_cast<const S*>(u2->data) : nullptr, r, partial);
+		return check_launch("k_reduce");
+	});
+	if (rc) return rc;
+	k_reduce_final<OP><<<1, kRedThreads, 0, s>>>(partial, blocks, result);
+	if ((rc = check_launch("k_reduce_final"))) return rc;
+	void* host;
+	if ((rc = host_staging(sizeof(double2), &host))) return rc;
+	if ((rc = cuda_error(cudaMemcpyAsync(host, result, sizeof(double2), cudaMemcpyDeviceToHost, s),
+				 "cudaMemcpyAsync(norm)")))
+		return rc;
+	if ((rc = cuda_error(cudaStreamSynchronize(s), "cudaStreamSynchronize(norm)"))) return rc;
+	const double2 v = *reinterpret_cast<double2*>(host);
+	if (out_a) *out_a = v.x;
+	if (out_b) *out_b = v.y;
+	return B200_OK;
+}
+
+int upload_tables(const b200_box* box, const double* v1, const double* v2, const double* v3,
+		cudaStream_t s, size_t offset_bytes, double** d1, double** d2, double** d3)
+{
+	if (!v1 || !v2 || !v3) return set_error(B200_ERR_ARG, "NULL table");
+	const size_t n1 = box->i1e - box->i1s + 1, n2 = box->i2e - box->i2s + 1,
+	             n3 = box->i3e - box->i3s + 1;
+	void* scr;
+	const size_t need = offset_bytes + (n1 + n2 + n3) * sizeof(double);
+	if (int rc = scratch(need, &scr)) return rc;
+	double* t = reinterpret_cast<double*>(static_cast<char*>(scr) + offset_bytes);
+	*d1 = t;
+	*d2 = t + n1;
+	*d3 = t + n1 + n2;
+	int rc = cuda_error(cudaMemcpyAsync(*d1, v1, n1 * sizeof(double), cudaMemcpyHostToDevice, s), "tables");
+	if (!rc) rc = cuda_error(cudaMemcpyAsync(*d2, v2, n2 * sizeof(double), cudaMemcpyHostToDevice, s), "tables");
+	if (!rc) rc = cuda_error(cudaMemcpyAsync(*d3, v3, n3 * sizeof(double), cudaMemcpyHostToDevice, s), "tables");
+	return rc;
+}
+
+}  // namespace
+
+// Host entry used by the propagator step (b200_stencil.cu).
+int apply_boundary(const b200_layout* lay, const b200_field& u, int bc_type, int faces,
+		cudaStream_t s)
+{
+	if (bc_type == B200_NO_BOUND_COND) return B200_OK;
+	if (bc_type != B200_BOUND_COND_ANTI_MIRROR)
+		return set_error(B200_ERR_ARG, "invalid boundary condition type %d", bc_type);
+	BcArgs a;
+	a.n1 = lay->n1;
+	a.n12 = lay->n1 * lay->n2;
+	a.s[0] = lay->s1; a.s[1] = lay->s2; a.s[2] = lay->s3;
+	a.e[0] = lay->e1; a.e[1] = lay->e2; a.e[2] = lay->e3;
+	a.halo = lay->halo;
+	a.dim = lay->dim;
+	a.faces = faces & 0x3F;
+	if (a.halo == 0 || a.faces == 0) return B200_OK;
+	bool small = false;
+	for (int d = 0; d < lay->dim; d++) small |= (a.e[d] - a.s[d] + 1) < (a.halo + 2);
+	return dispatch_dtype(u.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		S* p = static_cast<S*>(u.data);
+		if (small) {
+			for (int f = 0; f < 2 * lay->dim; f++) {
+				if (!(a.faces & (1 << f))) continue;
+				const int axis = f / 2;
+				const int64_t nx = a.e[0] - a.s[0] + 1, ny = a.e[1] - a.s[1] + 1,
+				              nz = a.e[2] - a.s[2] + 1;
+				const int64_t lines = (axis == 0) ? ny * nz : (axis == 1) ? nx * nz : nx * ny;
+				k_bc_face<S><<<(unsigned)((lines + 127) / 128), 128, 0, s>>>(p, a, f);
+				if (int rc = check_launch("k_bc_face")) return rc;
+			}
+			return B200_OK;
+		}
+		const int blocks = num_sms() * 4;
+		k_bc_halos<S><<<dim3(blocks, lay->dim), 256, 0, s>>>(p, a);
+		if (int rc = check_launch("k_bc_halos")) return rc;
+		k_bc_planes<S><<<dim3(blocks, lay->dim), 256, 0, s>>>(p, a);
+		return check_launch("k_bc_planes");
+	});
+}
+
+}  // namespace b200
+
+using namespace b200;
+
+extern "C" {
+
+int b200_fill_const(const b200_layout* lay, b200_field u, const b200_box* box, double val,
+		void* stream)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_box(lay, box)) return rc;
+	if (int rc = check_field(u, "u")) return rc;
+	const Box3 b = to_box3(box);
+	const double v = val / (double)u.scale;
+	return dispatch_dtype(u.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		S sv;
+		if constexpr (std::is_same_v<S, float>) sv = (float)v;
+		else if constexpr (std::is_same_v<S, double>) sv = v;
+		else if constexpr (std::is_same_v<S, __half>) sv = __double2half(v);
+		else sv = __double2bfloat16(v);
+		k_fill_const<S><<<row_grid(b), kRowThreads, 0, as_stream(stream)>>>(
+				static_cast<S*>(u.data), lay->n1, lay->n1 * lay->n2, b, sv);
+		return check_launch("k_fill_const");
+	});
+}
+
+int b200_fill_separable(const b200_layout* lay, b200_field u, const b200_box* box,
+		const double* v1, const double* v2, const double* v3, double amp, void* stream)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_box(lay, box)) return rc;
+	if (int rc = check_field(u, "u")) return rc;
+	cudaStream_t s = as_stream(stream);
+	double *d1, *d2, *d3;
+	if (int rc = upload_tables(box, v1, v2, v3, s, 0, &d1, &d2, &d3)) return rc;
+	const Box3 b = to_box3(box);
+	const double a = amp / (double)u.scale;
+	int rc = dispatch_dtype(u.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		k_fill_separable<S><<<row_grid(b), kRowThreads, 0, s>>>(static_cast<S*>(u.data), lay->n1,
+				lay->n1 * lay->n2, b, d1, d2, d3, a);
+		return check_launch("k_fill_separable");
+	});
+	if (rc) return rc;
+	// the tables live in the shared scratch buffer: keep them until the kernel has read them
+	return cuda_error(cudaStreamSynchronize(s), "cudaStreamSynchronize(fill)");
+}
+
+int b200_apply_boundary(const b200_layout* lay, b200_field u, int bc_type, int faces, void* stream)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_field(u, "u")) return rc;
+	return apply_boundary(lay, u, bc_type, faces, as_stream(stream));
+}
+
+int b200_update_pressure(const b200_layout* lay, b200_field prn, b200_field prc, b200_field coef,
+		b200_field lapla, void* stream)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_field(prn, "prn")) return rc;
+	if (int rc = check_field(prc, "prc")) return rc;
+	if (int rc = check_field(coef, "coef")) return rc;
+	if (int rc = check_field(lapla, "lapla")) return rc;
+	if (prc.dtype != prn.dtype || coef.dtype != prn.dtype || lapla.dtype != prn.dtype)
+		return set_error(B200_ERR_UNSUPPORTED, "updatePressure needs one storage type");
+	if (prn.scale != prc.scale || lapla.scale != prn.scale)
+		return set_error(B200_ERR_UNSUPPORTED, "prn, prc and lapla must share one scale");
+	const b200_box box{lay->s1, lay->e1, lay->s2, lay->e2, lay->s3, lay->e3};
+	const Box3 b = to_box3(&box);
+	return dispatch_dtype(prn.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		k_update_pressure<S, true><<<row_grid(b), kRowThreads, 0, as_stream(stream)>>>(
+				static_cast<S*>(prn.data), static_cast<const S*>(prc.data),
+				static_cast<const S*>(coef.data), static_cast<const S*>(lapla.data), lay->n1,
+				lay->n1 * lay->n2, b, coef.scale);
+		return check_launch("k_update_pressure");
+	});
+}
+
+int b200_sum_abs(const b200_layout* lay, b200_field u, const b200_box* box, double* out,
+		void* stream)
+{
+	RedArgs r{};
+	return run_reduce<RED_SUM_ABS>(lay, u, nullptr, box, r, out, nullptr, stream);
+}
+
+int b200_sum_abs_diff(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
+		double* out, void* stream)
+{
+	RedArgs r{};
+	return run_reduce<RED_L1>(lay, u1, &u2, box, r, out, nullptr, stream);
+}
+
+int b200_l1_sums(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
+		double* sum_abs_diff, double* sum_abs_ref, void* stream)
+{
+	RedArgs r{};
+	return run_reduce<RED_L1>(lay, u1, &u2, box, r, sum_abs_diff, sum_abs_ref, stream);
+}
+
+int b200_max_err(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
+		double max_err_float, double* out, void* stream)
+{
+	RedArgs r{};
+	r.max_err_float = max_err_float;
+	return run_reduce<RED_MAX_ERR>(lay, u1, &u2, box, r, out, nullptr, stream);
+}
+
+int b200_min_max(const b200_layout* lay, b200_field u, const b200_box* box, double* mn,
+		double* mx, void* stream)
+{
+	RedArgs r{};
+	return run_reduce<RED_MIN_MAX>(lay, u, nullptr, box, r, mn, mx, stream);
+}
+
+int b200_l1_sums_separable(const b200_layout* lay, b200_field u, const b200_box* box,
+		const double* v1, const double* v2, const double* v3, double amp, int ref_dtype,
+		double* sum_abs_diff, double* sum_abs_ref, void* stream)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_box(lay, box)) return rc;
+	if (dtype_size(ref_dtype) == 0) return set_error(B200_ERR_ARG, "ref dtype %d", ref_dtype);
+	RedArgs r{};
+	double *d1, *d2, *d3;
+	// tables after the partial sums in the scratch buffer
+	const size_t off = sizeof(double2) * (num_sms() * 8 + 1);
+	if (int rc = upload_tables(box, v1, v2, v3, as_stream(stream), (off + 255) & ~(size_t)255, &d1,
+				&d2, &d3))
+		return rc;
+	r.v1 = d1;
+	r.v2 = d2;
+	r.v3 = d3;
+	r.amp = amp;
+	r.ref_dtype = ref_dtype;
+	return run_reduce<RED_L1_SEP>(lay, u, nullptr, box, r, sum_abs_diff, sum_abs_ref, stream);
+}
+
+}  // extern "C"

@@ -16,11 +16,13 @@ Two layout policies are provided:
 * ``reference_layout``: exactly what the reference Grid builds, so that grids
   written by the reference (-writeGrid) can be read back;
 * ``b200_layout``: the layout Grid_B200 uses on the device. Grid lets a test
-  mode choose its own offset/padding (the protected virtual hooks
-  padGridn1..3 / offsetGridn1..3, src/grid.h:327-335). B200 starts the inner
-  points of every n1 row on a 16-byte boundary and makes the row pitch a
-  multiple of 32 bytes, which is what tensor-memory-accelerator (TMA) tile
-  loads require (16-byte aligned start coordinate and strides).
+  mode choose its own padding (the protected virtual hook padGridn1,
+  src/grid.h:327-335). B200 keeps the reference's offsets, so the inner points
+  sit at the same indices and get bit-identical coordinates (the origin is
+  derived from the inner start, src/grid.cpp:417 and :1924-1957), and pads n1
+  so that the row pitch is a multiple of 32 bytes: tensor-memory-accelerator
+  (TMA) tile loads need 16-byte strides, and the z-marching kernel tiles n1
+  from a 16-byte aligned index.
 """
 from __future__ import annotations
 
@@ -231,22 +233,12 @@ def reference_layout(dim: int, n1: int, n2: int = 1, n3: int = 1, order: int = 8
 
 def b200_layout(dim: int, n1: int, n2: int = 1, n3: int = 1, order: int = 8,
                 prec: str = "f32") -> GridLayout:
-    """The device layout of Grid_B200: inner start of each n1 row on a 16-byte
-    boundary (offset = -halo mod 16/elem), row pitch a multiple of 32 bytes."""
-    check_order(order)
-    h = halo_width(order)
-    es = ELEM_SIZE[prec]
-    a16 = 16 // es
-    a32 = 32 // es
-    off1 = (-h) % a16
-    ax1 = _axis(n1, h, off1)
-    n1_tot = -(-ax1.n // a32) * a32
-    ax1 = replace(ax1, n=n1_tot)
-    axes = [ax1]
-    for a, n in ((1, n2), (2, n3)):
-        axes.append(_axis(n, h, 0) if a + 1 <= dim else _FLAT_AXIS)
-    return GridLayout(dim=dim, order=order, prec=prec, a1=axes[0], a2=axes[1], a3=axes[2],
-                      n_inner=(n1, n2 if dim >= 2 else 1, n3 if dim >= 3 else 1))
+    """The device layout of Grid_B200: the reference's offsets, n1 padded to a
+    multiple of 32 bytes."""
+    ref = reference_layout(dim, n1, n2, n3, order=order, prec=prec)
+    a32 = 32 // ELEM_SIZE[prec]
+    n1_tot = -(-(ref.a1.halo2_end + 1) // a32) * a32
+    return replace(ref, a1=replace(ref.a1, n=n1_tot))
 
 
 # ---- coordinates and separable fills ----------------------------------------------------------

@@ -1,0 +1,181 @@
+/*
+ * hpcscan_b200 — C ABI of the B200 (sm_100a) implementation of the hpcscan
+ * finite-difference / acoustic-propagator hot path.
+ *
+ * This is the boundary a hpcscan test mode binds to: the C++ class Grid_B200
+ * (hpcscan_b200/host/grid_B200.cpp) subclasses the reference's Grid and
+ * forwards each virtual listed below to one of these entry points; any other
+ * host (Python ctypes, another C++ driver) can bind the same symbols.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only. Device pointers come from b200_malloc (or
+ *    any cudaMalloc'd memory of the current device).
+ *  - Every entry point returns an int status: B200_OK (0) or a negative code;
+ *    b200_last_error() returns a message for the calling thread. Nothing here
+ *    exits the process.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ *    stream). Kernels are enqueued on it; entry points that return host
+ *    scalars (the reductions) synchronise that stream.
+ *  - A grid is one flat array, i1 fastest: idx = i1 + i2*n1 + i3*n1*n2, with
+ *    the INNER box [s1,e1]x[s2,e2]x[s3,e3] (inclusive bounds) exactly as
+ *    Grid::getGridIndex(INNER_POINTS) returns it (reference src/grid.cpp:15-38,
+ *    2682-2843). For 1D and 2D grids the unused axes have n = 1 and s = e = 0.
+ *  - Arithmetic: FP32 storage computes in FP32 and FP64 in FP64, as the
+ *    reference's Myfloat/Myfloat2 builds do (src/type_def.h:22-44); FP16 and
+ *    BF16 storage compute in FP32. Norms accumulate in FP64.
+ *  - Field scale: a stored value s of a field with scale k stands for the
+ *    physical value s*k (a power of two for 16-bit storage, 1.0 otherwise).
+ */
+#ifndef HPCSCAN_B200_H_
+#define HPCSCAN_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------- */
+#define B200_OK               0
+#define B200_ERR_ARG         -1   /* invalid argument (size mismatch, bad order, bad box ...) */
+#define B200_ERR_CUDA        -2   /* a CUDA runtime/driver call failed                        */
+#define B200_ERR_UNSUPPORTED -3   /* valid but not supported (e.g. dtype for this operator)   */
+#define B200_ERR_TIMEOUT     -4   /* a bounded device-side wait ran out                       */
+#define B200_ERR_NOMEM       -5   /* device allocation failed                                 */
+
+/* ---- storage types ------------------------------------------------------------------------ */
+#define B200_F32  0
+#define B200_F64  1
+#define B200_F16  2
+#define B200_BF16 3
+
+/* ---- boundary conditions (reference src/type_def.h:99) ------------------------------------ */
+#define B200_NO_BOUND_COND          0
+#define B200_BOUND_COND_ANTI_MIRROR 1
+
+/* Array layout of one grid: full dims and the INNER box (inclusive), dim, halo = order/2. */
+typedef struct b200_layout {
+	int64_t n1, n2, n3;
+	int64_t s1, e1, s2, e2, s3, e3;
+	int32_t dim;
+	int32_t halo;
+} b200_layout;
+
+/* An index box, inclusive bounds (what Grid::getGridIndex returns for a point type). */
+typedef struct b200_box {
+	int64_t i1s, i1e, i2s, i2e, i3s, i3e;
+} b200_box;
+
+/* A field in device memory. */
+typedef struct b200_field {
+	void*   data;   /* device pointer, n1*n2*n3 elements                        */
+	int32_t dtype;  /* B200_F32 / B200_F64 / B200_F16 / B200_BF16               */
+	float   scale;  /* physical value = stored value * scale                    */
+} b200_field;
+
+/* ---- runtime -------------------------------------------------------------------------------
+ * b200_init: select the device (reference: cudaSetDevice(rank % deviceCount) in
+ * Grid_Cuda::initializeGrid, src/grid_Cuda.cu:2757-2762) and prepare the per-device state. */
+int         b200_init(int device);
+const char* b200_last_error(void);
+int         b200_device_count(int* count);
+int         b200_malloc(void** dptr, size_t bytes);
+int         b200_free(void* dptr);
+int         b200_memcpy_h2d(void* dst, const void* src, size_t bytes, void* stream);
+int         b200_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream);
+int         b200_memcpy_d2d(void* dst, const void* src, size_t bytes, void* stream);
+int         b200_memset(void* dptr, int value, size_t bytes, void* stream);
+int         b200_stream_sync(void* stream);
+/* Copy one box of a grid between host and device (the rest untouched); replaces the
+ * host<->device staging of Grid_Cuda::copyGridDeviceToHost/HostToDevice
+ * (src/grid_Cuda.cu:3410-3470). elem_size = bytes per element. */
+int         b200_copy_box_d2h(const b200_layout* lay, int elem_size, void* host, const void* dev,
+		const b200_box* box, void* stream);
+int         b200_copy_box_h2d(const b200_layout* lay, int elem_size, void* dev, const void* host,
+		const b200_box* box, void* stream);
+
+/* ---- fills ---------------------------------------------------------------------------------
+ * Grid::fill(pointType, val) (src/grid.cpp:1808-1826). */
+int b200_fill_const(const b200_layout* lay, b200_field u, const b200_box* box, double val,
+		void* stream);
+
+/* Grid::fill(pType, f1, f2, f3, p1, p2, p3, amp) (src/grid.cpp:1650-1805): the caller
+ * supplies the three FP64 1-D tables v1[i1-i1s], v2[i2-i2s], v3[i3-i3s] (host memory);
+ * u = (stored type)(amp * v1 * v2 * v3 / u.scale) over the box. */
+int b200_fill_separable(const b200_layout* lay, b200_field u, const b200_box* box,
+		const double* v1, const double* v2, const double* v3, double amp, void* stream);
+
+/* ---- finite-difference operators (INNER points; `u` in, `w` out) ----------------------------
+ * inv2_a = (1/d_a)^2 evaluated in the compute type by the caller (src/grid.cpp:3252-3258).
+ * Grid::FD_D2_N1/N2/N3 (src/grid.cpp:3232, 3566, 3900); axis = 1, 2 or 3. */
+int b200_fd_d2(const b200_layout* lay, int axis, int order, b200_field u, b200_field w,
+		double inv2_1, double inv2_2, double inv2_3, void* stream);
+
+/* Grid::FD_LAPLACIAN (src/grid.cpp:4235-4576). */
+int b200_laplacian(const b200_layout* lay, int order, b200_field u, b200_field w,
+		double inv2_1, double inv2_2, double inv2_3, void* stream);
+
+/* Grid::updatePressure (src/grid.cpp:4579-4609): prn = 2 prc - prn + coef*lapla, INNER. */
+int b200_update_pressure(const b200_layout* lay, b200_field prn, b200_field prc, b200_field coef,
+		b200_field lapla, void* stream);
+
+/* Grid::computePressureWithFD (src/grid.cpp:4612-5113), `this` = prn:
+ * prn = 2 prc - prn + coef * Laplacian(prc) on INNER points, in one pass. */
+int b200_compute_pressure(const b200_layout* lay, int order, b200_field prn, b200_field prc,
+		b200_field coef, double inv2_1, double inv2_2, double inv2_3, void* stream);
+
+/* Grid::applyBoundaryCondition (src/grid.cpp:3065-3229). `faces` is a 6-bit mask of the
+ * faces with no neighbour (bit 0: I1HALO1, 1: I1HALO2, 2: I2HALO1, 3: I2HALO2,
+ * 4: I3HALO1, 5: I3HALO2); 0x3F for a single rank. Same result as the reference's
+ * sequential face order. */
+int b200_apply_boundary(const b200_layout* lay, b200_field u, int bc_type, int faces,
+		void* stream);
+
+/* Propagator_Ac2::computeWavefieldNextTimeStep for one rank (src/propagator_Ac2.cpp:366-395):
+ * applyBoundaryCondition(prc) then computePressureWithFD(prn, prc), in one call. */
+int b200_propagate_step(const b200_layout* lay, int order, b200_field prn, b200_field prc,
+		b200_field coef, double inv2_1, double inv2_2, double inv2_3, int bc_type, void* stream);
+
+/* ---- norms (FP64 accumulation; synchronous on `stream`) ------------------------------------
+ * Grid::getSumAbs (src/grid.cpp:2230-2273). */
+int b200_sum_abs(const b200_layout* lay, b200_field u, const b200_box* box, double* out,
+		void* stream);
+/* Grid::getSumAbsDiff (src/grid.cpp:2176-2227): sum |u1 - u2|. */
+int b200_sum_abs_diff(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
+		double* out, void* stream);
+/* Grid::L1Err (src/grid.cpp:2058-2110) in one pass: sum |u1 - u2| and sum |u2|. */
+int b200_l1_sums(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
+		double* sum_abs_diff, double* sum_abs_ref, void* stream);
+/* Grid::maxErr (src/grid.cpp:2006-2055): max over the box of |u1-u2|/|u2|, or |u1-u2|
+ * where |(float)u2| < max_err_float (MAX_ERR_FLOAT, src/constant.h:14-20). */
+int b200_max_err(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
+		double max_err_float, double* out, void* stream);
+/* Grid::getMin / getMax (src/grid.cpp:2276-2336), both in one pass. */
+int b200_min_max(const b200_layout* lay, b200_field u, const b200_box* box, double* mn,
+		double* mx, void* stream);
+
+/* Analytic-reference error norm without materialising the reference grid: the
+ * separable field r = amp*v1*v2*v3 (rounded to u's storage type, as Grid::fill would
+ * store it) replaces u2 in b200_l1_sums. This fuses the refGrid fill + getSumAbsDiff +
+ * getSumAbs of TestCase_Propa::run (src/testCase_Propa.cpp:136-151) into one read of u. */
+int b200_l1_sums_separable(const b200_layout* lay, b200_field u, const b200_box* box,
+		const double* v1, const double* v2, const double* v3, double amp, int ref_dtype,
+		double* sum_abs_diff, double* sum_abs_ref, void* stream);
+
+/* ---- diagnostics ----------------------------------------------------------------------------
+ * Device-side error word of the library's kernels (0 = none; bit 0: a producer gave up a
+ * bounded wait, bit 1: a consumer did). Synchronous; `clear` resets it. No reference
+ * counterpart: the reference's CUDA modes have no device-side waits. */
+int b200_device_status(int* status, int clear);
+
+/* Which kernel family computes a stencil call with this layout/order/dtype on the current
+ * device: 1 = 3-D z-marching TMA kernel, 2 = direct kernel, 0 = rejected (see
+ * b200_last_error). No device work. No reference counterpart. */
+int b200_stencil_route(const b200_layout* lay, int order, int dtype, int* route);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPCSCAN_B200_H_ */

@@ -1,0 +1,267 @@
+"""GPU parity of the hpcscan_b200 kernels against the oracle (oracle/oracle.c, itself
+pinned to the reference) and against the reference-written golden grids.
+
+Elementwise results (fills, FD_D2, Laplacian, pressure update, boundary condition)
+must be BIT-IDENTICAL in FP32 and FP64: the kernels evaluate the reference's
+expressions in its order with separately rounded operations. FP64 norms are
+compared at 1e-12 relative (summation order differs).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from hpcscan_b200 import layout as L  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+MANIFEST = json.load(open(os.path.join(GOLDEN, "manifest.json")))
+ORDERS = (2, 4, 6, 8, 10, 12, 14, 16)
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hpcscan_b200.grid import init_device
+    init_device(0)
+    return torch
+
+
+def dev(lay, arr=None, samp=None):
+    from hpcscan_b200.grid import Grid
+    g = Grid(lay, samp)
+    g.initializeGrid()
+    if arr is not None:
+        g.from_numpy(arr)
+    return g
+
+
+def rand_field(lay, seed):
+    rng = np.random.default_rng(seed)
+    t = np.float32 if lay.prec == "f32" else np.float64
+    return rng.uniform(-1.0, 1.0, lay.npoint).astype(t)
+
+
+def bits(a):
+    return a.view(np.uint32 if a.dtype == np.float32 else np.uint64)
+
+
+def layouts():
+    """3-D layouts exercising both kernel families (the B200 layout goes to the z-marching
+    TMA kernel; the reference layout, whose row pitch is not a multiple of 16 bytes, to
+    the direct kernel), with several tiles and z-chunks and partial edge tiles, plus 1-D
+    and 2-D."""
+    out = []
+    for prec in ("f32", "f64"):
+        for o in ORDERS:
+            out.append(L.b200_layout(3, 37, 20, 23, order=o, prec=prec))
+        out.append(L.b200_layout(3, 130, 37, 150, order=8, prec=prec))
+        out.append(L.b200_layout(3, 70, 33, 41, order=16, prec=prec))
+        out.append(L.b200_layout(3, 77, 45, 70, order=2, prec=prec))
+        out.append(L.reference_layout(3, 29, 21, 20, order=6, prec=prec))
+        out.append(L.reference_layout(3, 31, 21, 20, order=8, prec=prec))
+        out.append(L.reference_layout(2, 40, 33, order=12, prec=prec))
+        out.append(L.reference_layout(1, 57, order=16, prec=prec))
+    return out
+
+
+def lay_id(lay):
+    return f"d{lay.dim}_o{lay.order}_{lay.prec}_{lay.n1}x{lay.n2}x{lay.n3}"
+
+
+def route(lay):
+    import ctypes
+    from hpcscan_b200 import _lib
+    r = ctypes.c_int()
+    cl = _lib.Layout(*lay.c_struct_fields())
+    _lib.call("b200_stencil_route", ctypes.byref(cl), lay.order, _lib.DTYPE_CODE[lay.prec],
+              ctypes.byref(r))
+    return r.value
+
+
+def device_status():
+    import ctypes
+    from hpcscan_b200 import _lib
+    st = ctypes.c_int()
+    _lib.call("b200_device_status", ctypes.byref(st), 1)
+    return st.value
+
+
+def test_routes(gpu):
+    """The B200 layout of every 3-D FP32/FP64 grid takes the z-marching TMA kernel."""
+    for prec in ("f32", "f64"):
+        for o in ORDERS:
+            assert route(L.b200_layout(3, 37, 20, 23, order=o, prec=prec)) == 1
+        assert route(L.b200_layout(2, 37, 20, order=8, prec=prec)) == 2
+    # row pitch not a multiple of 16 bytes: direct kernel
+    assert route(L.reference_layout(3, 29, 21, 20, order=6, prec="f64")) == 2
+    assert route(L.reference_layout(3, 31, 21, 20, order=8)) == 2
+
+
+@pytest.mark.parametrize("lay", layouts(), ids=lay_id)
+def test_fd_operators_bitexact(gpu, oracle, lay):
+    u = rand_field(lay, 1)
+    samp = L.Sampling((0.013, 0.011, 0.017), (0.0, 0.0, 0.0))
+    inv2 = L.inv2_spacing(samp, lay.prec)
+    U = dev(lay, u, samp)
+    for axis in range(0, lay.dim + 1):
+        W = dev(lay, None, samp)
+        w_ref = oracle.alloc(lay)
+        if axis == 0:
+            assert U.FD_LAPLACIAN(L.INNER_POINTS, W, lay.order) == 0
+            oracle.laplacian(lay, u, w_ref, inv2)
+        else:
+            assert getattr(U, f"FD_D2_N{axis}")(L.INNER_POINTS, W, lay.order) == 0
+            oracle.fd_d2(lay, axis, u, w_ref, inv2)
+        got = W.to_numpy()
+        assert np.array_equal(bits(got), bits(w_ref)), (axis, np.abs(got - w_ref).max())
+    assert device_status() == 0
+
+
+@pytest.mark.parametrize("lay", layouts(), ids=lay_id)
+def test_compute_pressure_bitexact(gpu, oracle, lay):
+    prc, prn, coef = rand_field(lay, 2), rand_field(lay, 3), np.abs(rand_field(lay, 4)) * 1e-3
+    samp = L.Sampling((0.02, 0.03, 0.025), (0.0, 0.0, 0.0))
+    inv2 = L.inv2_spacing(samp, lay.prec)
+    Prc, Prn, Coef = dev(lay, prc, samp), dev(lay, prn, samp), dev(lay, coef, samp)
+    assert Prn.computePressureWithFD(Prc, Coef, lay.order) == 0
+    ref = prn.copy()
+    oracle.compute_pressure(lay, ref, prc, coef, inv2)
+    got = Prn.to_numpy()
+    assert np.array_equal(bits(got), bits(ref)), np.abs(got - ref).max()
+    assert device_status() == 0
+    # the input is untouched
+    assert np.array_equal(bits(Prc.to_numpy()), bits(prc))
+
+
+@pytest.mark.parametrize("lay", layouts(), ids=lay_id)
+def test_update_pressure_bitexact(gpu, oracle, lay):
+    a = [rand_field(lay, s) for s in (5, 6, 7, 8)]
+    G = [dev(lay, x) for x in a]
+    assert G[0].updatePressure(L.INNER_POINTS, G[1], G[2], G[3]) == 0
+    ref = a[0].copy()
+    oracle.update_pressure(lay, ref, a[1], a[2], a[3])
+    assert np.array_equal(bits(G[0].to_numpy()), bits(ref))
+
+
+BC_LAYOUTS = [L.b200_layout(3, 30, 21, 22, order=8), L.reference_layout(3, 25, 20, 21, order=16),
+              L.b200_layout(3, 12, 9, 10, order=16, prec="f64"),      # small: sequential faces
+              L.reference_layout(2, 33, 20, order=4, prec="f64"), L.reference_layout(1, 40, order=6)]
+
+
+@pytest.mark.parametrize("lay", BC_LAYOUTS, ids=lay_id)
+def test_boundary_condition_bitexact(gpu, oracle, lay):
+    """Anti-mirror BC: same bits as the reference's sequential faces, signs of zero included."""
+    u = rand_field(lay, 9)
+    U = dev(lay, u)
+    assert U.applyBoundaryCondition() == 0
+    ref = u.copy()
+    oracle.apply_bc(lay, ref)
+    assert np.array_equal(bits(U.to_numpy()), bits(ref))
+
+
+@pytest.mark.parametrize("lay", BC_LAYOUTS[:2] + [L.b200_layout(3, 41, 33, 20, order=8, prec="f64")],
+                         ids=lay_id)
+def test_norms(gpu, oracle, lay):
+    u1, u2 = rand_field(lay, 10), rand_field(lay, 11)
+    A, B = dev(lay, u1), dev(lay, u2)
+    for pt in (L.INNER_POINTS, L.ALL_POINTS, L.I1HALO1, L.I3INNERHALO2):
+        box = lay.box(pt)
+        np.testing.assert_allclose(A.getSumAbs(pt), oracle.sum_abs(lay, u1, box), rtol=1e-12)
+        np.testing.assert_allclose(A.getSumAbsDiff(pt, B), oracle.sum_abs_diff(lay, u1, u2, box),
+                                   rtol=1e-12)
+        np.testing.assert_allclose(A.maxErr(pt, B), oracle.max_err(lay, u1, u2, box), rtol=1e-15)
+        mn, mx = oracle.min_max(lay, u1, box)
+        assert A.getMin(pt) == mn and A.getMax(pt) == mx
+    np.testing.assert_allclose(A.L1Err(L.INNER_POINTS, B),
+                               oracle.l1_err(lay, u1, u2, lay.box(L.INNER_POINTS)), rtol=1e-12)
+
+
+def test_size_mismatch_and_bad_arguments(gpu):
+    from hpcscan_b200 import _lib
+    a = dev(L.b200_layout(3, 20, 20, 20, order=8))
+    b = dev(L.b200_layout(3, 20, 21, 20, order=8))
+    assert a.FD_LAPLACIAN(L.INNER_POINTS, b, 8) == -1            # RTN_CODE_KO
+    assert a.getSumAbsDiff(L.INNER_POINTS, b) == -1.0
+    assert a.L1Err(L.INNER_POINTS, b) == -1.0
+    assert a.applyBoundaryCondition(7) == -1
+    with pytest.raises(_lib.B200Error):
+        a.FD_LAPLACIAN(L.INNER_POINTS, dev(a.layout), 6)        # halo/order mismatch
+    with pytest.raises(ValueError):
+        a.FD_D2_N1(L.INNER_POINTS, dev(a.layout), 5)
+
+
+# ---- golden fixtures written by the reference ---------------------------------------------------
+
+FD_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "FD_D2")
+PROPA_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "Propa")
+
+
+def flag_value(flags, name, default):
+    return float(flags[flags.index(name) + 1]) if name in flags else default
+
+
+@pytest.mark.parametrize("fixture", FD_FIXTURES)
+def test_fd_golden_on_gpu(gpu, fixture):
+    """Unchanged FD_D2 test-case inputs in the B200 layout: fill and every operator give the
+    reference's inner values bit for bit."""
+    meta = MANIFEST[fixture]
+    gold = np.load(os.path.join(GOLDEN, fixture))
+    flags = meta["flags"]
+    lay = L.b200_layout(meta["dim"], *meta["n"], order=meta["order"], prec=meta["prec"])
+    ref_lay = L.reference_layout(meta["dim"], *meta["n"], order=meta["order"], prec=meta["prec"])
+    p = [flag_value(flags, f"-param{i + 1}", (0.8, 0.9, 1.0, 1.1)[i]) for i in range(4)]
+    U = dev(lay)
+    U.defineUnitGrid()
+    U.fill(L.ALL_POINTS, L.FUNC_SINE, L.FUNC_SINE, L.FUNC_SINE, L.PI * p[0], L.PI * p[1],
+           L.PI * p[2], p[3])
+    if "U" in gold and not any("Pad" in f for f in flags):
+        # the fill is independent of padding: compare the inner points
+        assert np.array_equal(lay.inner(U.to_numpy()), ref_lay.inner(gold["U"]))
+    for case in meta["cases"]:
+        W = dev(lay)
+        W.defineUnitGrid()
+        if case.startswith("Axis"):
+            getattr(U, f"FD_D2_N{case[-1]}")(L.INNER_POINTS, W, meta["order"])
+        else:
+            U.FD_LAPLACIAN(L.INNER_POINTS, W, meta["order"])
+        assert np.array_equal(lay.inner(W.to_numpy()), gold[case]), case
+
+
+@pytest.mark.parametrize("fixture", PROPA_FIXTURES)
+def test_propa_golden_on_gpu(gpu, fixture):
+    """The Propa test case (standard and split propagators) on the GPU reproduces the
+    reference's wavefields bit for bit at every check, and its errTestCase."""
+    from hpcscan_b200.propagator import run_propa
+    meta = MANIFEST[fixture]
+    gold = np.load(os.path.join(GOLDEN, fixture))
+    flags = meta["flags"]
+    lay = L.b200_layout(meta["dim"], *meta["n"], order=meta["order"], prec=meta["prec"])
+    got = []
+    res = run_propa(lay, propagator=meta["propagator"],
+                    ratio_cfl=flag_value(flags, "-ratioCFL", 1.0),
+                    nt=int(flag_value(flags, "-nt", 20)),
+                    snap_inc=int(flag_value(flags, "-snapInc", 1)),
+                    modes=tuple(flag_value(flags, f"-param{i + 1}", (0.8, 0.9, 1.0)[i])
+                                for i in range(3)),
+                    on_check=lambda it, prn, ref: got.append(lay.inner(prn.to_numpy())))
+    assert res.nt == meta["nt"]
+    for i, g in enumerate(got):
+        assert np.array_equal(g, gold[f"prn_{i}"]), i
+    assert abs(res.err_test_case - meta["err_test_case"]) <= 2e-5 * abs(meta["err_test_case"])
+
+
+def test_fused_check_equals_materialised_reference(gpu):
+    """b200_l1_sums_separable gives the sums of fill + getSumAbsDiff + getSumAbs."""
+    from hpcscan_b200.propagator import run_propa
+    lay = L.b200_layout(3, 40, 36, 33, order=8)
+    a = run_propa(lay, nt=12, snap_inc=3, fused_check=True)
+    b = run_propa(lay, nt=12, snap_inc=3, fused_check=False)
+    for (ia, s1a, s2a), (ib, s1b, s2b) in zip(a.checks, b.checks):
+        assert ia == ib
+        np.testing.assert_allclose([s1a, s2a], [s1b, s2b], rtol=1e-12)
+    assert a.err_test_case == b.err_test_case

@@ -150,10 +150,13 @@ def test_layouts_match_reference_rules():
     lay = L.reference_layout(3, 21, 20, 20, order=6, prec="f64")
     assert lay.a1.inner_start == 3
     b = L.b200_layout(3, 512, 512, 512, order=8)
-    assert b.a1.inner_start % 4 == 0 and (b.n1 * 4) % 32 == 0
+    assert b.a1.inner_start == 4 and b.n1 == 520 and (b.n1 * 4) % 32 == 0
     for o in (2, 4, 6, 8, 10, 12, 14, 16):
-        for prec, al in (("f32", 4), ("f64", 2), ("f16", 8), ("bf16", 8)):
+        for prec in ("f32", "f64", "f16", "bf16"):
             b = L.b200_layout(3, 33, 20, 21, order=o, prec=prec)
-            assert b.a1.inner_start % al == 0
+            r = L.reference_layout(3, 33, 20, 21, order=o, prec=prec)
+            # same inner indices (hence the same coordinates) as the reference grid
+            assert b.box(L.INNER_POINTS) == r.box(L.INNER_POINTS)
+            assert b.box(L.ALL_POINTS) == r.box(L.ALL_POINTS)
             assert (b.n1 * b.elem_size) % 32 == 0
-            assert b.a1.halo2_end < b.n1
+            assert b.n1 >= r.n1 and (b.n2, b.n3) == (r.n2, r.n3)
