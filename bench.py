@@ -1,0 +1,417 @@
+"""Benchmark of the hpcscan B200 hot path: the Propa acoustic propagator step.
+
+Workload (BASELINE north-star configuration): Propa Ac2Standard, FD order 8, FP32,
+n1 = n2 = n3 = 512 inner points (520^3 with halos), eigen mode (1, 1, 1), ratioCFL 0.8.
+A step is one time step of Propagator_Ac2::computeWavefieldNextTimeStep:
+applyBoundaryCondition(prc) then computePressureWithFD(prn, prc), then the swap.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--size 512]
+
+One JSON line on stdout (rank 0). Under torchrun every rank runs its own replica of the
+workload on its GPU (the propagator does not shard on one grid: "replicas only"), the
+device time is the max over ranks, and value = all points updated / that time.
+
+  value          GPoint/s with the grids resident in HBM (device time, CUDA events)
+  e2e            GPoint/s of one whole Propa job through the Python Grid/propagator API:
+                 host eigen-mode fields (pinned) -> device, nt time steps with the
+                 reference's periodic analytic checks, final wavefield -> host
+  roofline       the fused pressure kernel: 16 algorithmic bytes per inner point
+                 (prc, prn, coef read once, prn written once) / its mean launch time,
+                 against the measured HBM copy bandwidth
+  cpu_baseline   the reference CPU path itself (oracle/_ref/hpcscan_fp32, test mode
+                 CacheBlk, all host threads) on a bounded number of steps of the same grid
+--impl reference prints the same line for the reference CPU implementation.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+METRIC = "Propa GPoint/s (O8 FP32 acoustic leapfrog step, 512^3)"
+UNIT = "GPoint/s"
+ALG_BYTES_PER_POINT = 16     # FP32: read prc, prn, coef; write prn (computePressureWithFD)
+KERNEL_NAME = "k_zmarch (computePressureWithFD, TMA z-marching)"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--size", type=int, default=512)
+    p.add_argument("--order", type=int, default=8)
+    p.add_argument("--e2e-steps", type=int, default=0,
+                   help="time steps of the end-to-end job (default: one period of the mode)")
+    p.add_argument("--cpu-steps", type=int, default=200,
+                   help="time steps of the bounded reference CPU sample")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the pressure kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "zmarch_pressure_o8_f32_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- reference CPU path -------------------------------------------------------------------------
+
+def run_reference_cpu(n: int, order: int, nt: int, threads: int):
+    """Run the reference Propa test case (CacheBlk) for nt steps and return its own
+    timers: (GPoint/s over BC + pressure time, details)."""
+    from oracle import oracle
+    exe = oracle.ref_binary("f32")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    args = [exe, "-testCase", "Propa", "-testMode", "CacheBlk", "-propagator", "Ac2Standard",
+            "-fdOrder", str(order), "-n1", str(n), "-n2", str(n), "-n3", str(n),
+            "-ratioCFL", "0.8", "-param1", "1", "-param2", "1", "-param3", "1",
+            "-nt", str(nt), "-snapInc", str(nt), "-ntry", "1"]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        out = subprocess.run(args, cwd=d, capture_output=True, text=True, env=env, timeout=900)
+        wall = time.perf_counter() - t0
+    if out.returncode != 0:
+        raise RuntimeError(out.stdout[-2000:] + out.stderr[-2000:])
+    txt = out.stdout
+
+    def grab(pat):
+        m = re.search(pat + r"\s+(\S+)", txt)
+        return float(m.group(1)) if m else None
+    t_bc = grab(r"Bound\. cond\. time \(s\)")
+    t_p = grab(r"Compute pres\. time \(s\)")
+    pts = float(n) ** 3 * nt
+    value = pts / (t_bc + t_p) / 1e9
+    return value, {"bc_s": t_bc, "pressure_s": t_p, "gpoint_fd": grab(r"Best Gpoint/s in FD"),
+                   "wall_s": wall, "nt": nt}
+
+
+def reference_arm(a):
+    rank, world, _ = dist_env()
+    if world > 1 and rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    nt = max(a.steps, 1)
+    try:
+        value, det = run_reference_cpu(a.size, a.order, nt, threads)
+    except Exception as e:   # the reference binary is built by build(); report why not
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU run failed: {e}"[:300]}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+        "n_gpus": a.gpus, "steps": nt, "warmup": 0,
+        "ms_per_step": round((det["bc_s"] + det["pressure_s"]) / nt * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (eigen mode, the reference's own Propa initialisation)",
+        "config": {"workload": f"Propa Ac2Standard O{a.order} FP32 {a.size}^3 eigen mode",
+                   "n": a.size, "order": a.order, "ratio_cfl": 0.8,
+                   "test_mode": "CacheBlk (reference CPU, unchanged source)"},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{nt} time steps of {a.size}^3, timed by the reference's own "
+                                   "boundary-condition + compute-pressure timers"},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "details": det,
+    }
+    print(json.dumps(line))
+
+
+# ---- B200 arm ------------------------------------------------------------------------------------
+
+def b200_arm(a):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from hpcscan_b200 import _lib
+    from hpcscan_b200 import layout as L
+    from hpcscan_b200.grid import Grid, init_device
+    from hpcscan_b200.propagator import Propagator_Ac2, run_propa
+
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local}"))
+    init_device(local)
+    lay = L.b200_layout(3, a.size, a.size, a.size, order=a.order, prec="f32")
+
+    propa = Propagator_Ac2(lay, device=local)
+    propa.initialize(ratio_cfl=0.8, nt=1, snap_inc=1, modes=(1, 1, 1))
+    prn, prc = propa.prnGrid, propa.prcGrid
+    stream = torch.cuda.current_stream()
+
+    # events around every pressure-kernel launch of the timed region (same stream)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(a.steps)]
+
+    def step(i=None):
+        nonlocal prn, prc
+        prc.applyBoundaryCondition()
+        if i is not None:
+            kev[i][0].record(stream)
+        propa.computePressureWithFD(prn, prc)
+        if i is not None:
+            kev[i][1].record(stream)
+        prn, prc = prc, prn
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(a.steps):
+            step(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kern_ms = [s.elapsed_time(e) for s, e in kev]
+    st = ctypes.c_int()
+    _lib.call("b200_device_status", ctypes.byref(st), 1)
+    if st.value:
+        raise RuntimeError(f"device-side error word {st.value}")
+    if dist is not None:
+        t = torch.tensor([ms, statistics.mean(kern_ms)], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, kmean = t.tolist()
+    else:
+        kmean = statistics.mean(kern_ms)
+    pts = lay.inner_points
+    value = world * pts * a.steps / (ms * 1e-3) / 1e9
+
+    # error of the benchmarked field against the analytic solution at the last step
+    del kev
+    peak, peak_src = measured_peak()
+    achieved = ALG_BYTES_PER_POINT * pts / (kmean * 1e-3) / 1e9
+    traffic = profiled_traffic()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_src,
+            "kernel": KERNEL_NAME, "kernel_ms": round(kmean, 5),
+            "alg_bytes_per_point": ALG_BYTES_PER_POINT, "points_per_launch": pts,
+            "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch_scaled"),
+            "traffic_note": None if traffic is None else traffic.get("note")}
+    # free the timed grids before the end-to-end job
+    del propa, prn, prc
+    torch.cuda.empty_cache()
+
+    e2e = e2e_job(a, lay, local)
+    if dist is not None:
+        t = torch.tensor([e2e["seconds"]], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e["value"] = round(world * e2e["points"] / t.item() / 1e9, 4)
+
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        threads = os.cpu_count() or 1
+        try:
+            v, det = run_reference_cpu(a.size, a.order, a.cpu_steps, threads)
+            cpu = {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{a.cpu_steps} time steps of the same {a.size}^3 O{a.order} FP32 "
+                             "Propa grid, reference CacheBlk, timed by its own BC + pressure timers",
+                   "details": det}
+        except Exception as e:
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"unavailable: {e}"[:200]}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (eigen mode sin(pi x) sin(pi y) sin(pi z), the reference's Propa "
+                "initialisation; no dataset involved)",
+        "config": {"workload": f"Propa Ac2Standard O{a.order} FP32 {a.size}^3 eigen mode "
+                               "(BC + fused pressure update per step)",
+                   "n": a.size, "order": a.order, "ratio_cfl": 0.8, "layout_n1": lay.n1,
+                   "l2": "inputs larger than L2 (3 x %.0f MB grids vs 126 MB L2)" % (lay.nbytes / 1e6),
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": 3 * a.steps,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step",
+                                    "job_steps", "err_test_case", "note")},
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
+def e2e_job(a, lay, device):
+    """One Propa job through the public API from host memory: the initial fields are
+    built on the host (as a caller holding its own arrays would), copied from pinned
+    memory into the grids, the time loop runs with the reference's analytic checks
+    (every snapInc steps, fused norm), and the final wavefield comes back to the host."""
+    import numpy as np
+    import torch
+
+    from hpcscan_b200 import layout as L
+    from hpcscan_b200.propagator import Propagator_Ac2, l1_sums_eigen
+    from hpcscan_b200.propa_setup import EIGEN_FUNCS, eigen_setup, init_times
+
+    setup = eigen_setup(lay, ratio_cfl=0.8, tmax=2.0 / np.sqrt(3.0), modes=(1, 1, 1))
+    nt = a.e2e_steps if a.e2e_steps > 0 else setup.nt
+    snap = max(1, nt // 10)
+    # host inputs (pinned): prn(-2dt), prc(-dt), coef
+    samp = setup.samp
+    tabs = L.fill_tables(lay, samp, L.ALL_POINTS, EIGEN_FUNCS, setup.params(lay))
+    t_prn, t_prc = init_times(setup, "f32")
+    sh = lay.shape3
+    b = lay.box(L.ALL_POINTS)
+
+    def host_field(amp):
+        h = torch.zeros(lay.npoint, dtype=torch.float32).pin_memory()
+        v = h.numpy().reshape(sh)
+        sl = lay.box_slices(L.ALL_POINTS)
+        # (((amp * v1) * v2) * v3) per point, the order of Grid::fill
+        v[sl] = (((amp * tabs[0][None, None, :]) * tabs[1][None, :, None]) *
+                 tabs[2][:, None, None]).astype(np.float32)
+        return h
+    h_prn = host_field(setup.amplitude(t_prn))
+    h_prc = host_field(setup.amplitude(t_prc))
+    h_coef = torch.zeros(lay.npoint, dtype=torch.float32).pin_memory()
+    h_coef.numpy().reshape(sh)[lay.box_slices(L.INNER_POINTS)] = np.float32(setup.coef)
+    h_out = torch.empty(lay.npoint, dtype=torch.float32).pin_memory()
+
+    propa = Propagator_Ac2(lay, device=device)
+    propa.initialize(ratio_cfl=0.8, tmax=2.0 / np.sqrt(3.0), modes=(1, 1, 1))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    prn, prc = propa.prnGrid, propa.prcGrid
+    prn.data.copy_(h_prn, non_blocking=True)
+    prc.data.copy_(h_prc, non_blocking=True)
+    propa.coefGrid.data.copy_(h_coef, non_blocking=True)
+    sum1 = np.float32(0)
+    sum2 = np.float32(0)
+    for it in range(nt):
+        propa.computeWavefieldNextTimeStep(prn, prc)
+        if it % snap == 0:
+            s1, s2 = l1_sums_eigen(prn, propa, setup.amplitude(setup.time_of_step(it, "f32")))
+            sum1 = np.float32(sum1 + np.float32(s1))
+            sum2 = np.float32(sum2 + np.float32(s2))
+        prn, prc = prc, prn
+    h_out.copy_(prc.data, non_blocking=True)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    pts = lay.inner_points * nt
+    h2d = 3 * lay.nbytes
+    d2h = lay.nbytes + (nt // snap + 1) * 16
+    return {"value": round(pts / sec / 1e9, 4), "unit": UNIT, "seconds": sec, "points": pts,
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "job_steps": nt,
+            "err_test_case": float(np.float32(sum1 / sum2)),
+            "note": "one e2e step = one whole Propa job of job_steps time steps from pinned "
+                    "host arrays (H2D of prn, prc, coef; D2H of the final wavefield and of "
+                    "the periodic analytic-check norms)"}
+
+
+def main():
+    a = parse_args()
+    if a.impl == "reference":
+        reference_arm(a)
+    else:
+        b200_arm(a)
+
+
+if __name__ == "__main__":
+    main()

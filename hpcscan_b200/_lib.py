@@ -83,7 +83,14 @@ SIGNATURES = {
     "b200_l1_sums_separable": [_PL, Field, _PB, _VP, _VP, _VP, _D, _I, _PD, _PD, _VP],
     "b200_device_status": [ctypes.POINTER(_I), _I],
     "b200_stencil_route": [_PL, _I, _I, ctypes.POINTER(_I)],
+    "b200_set_arith_mode": [_I],
+    "b200_get_arith_mode": [ctypes.POINTER(_I)],
+    "b200_set_stencil_config": [_I, _I, _I, _I, _I],
+    "b200_get_stencil_config": [_I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "b200_autotune_stencil": [_PL, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), _PD],
 }
+B200_ARITH_EXACT, B200_ARITH_FMA = 0, 1
+OP_FD_D2_N1, OP_FD_D2_N2, OP_FD_D2_N3, OP_LAPLACIAN, OP_PRESSURE, OP_STEP = 1, 2, 3, 4, 5, 6
 _RESTYPE = {"b200_last_error": ctypes.c_char_p}
 
 _lib = None

@@ -61,110 +61,116 @@ struct BcArgs {
 // I1HALO1, I1HALO2, I2HALO1, I2HALO2, I3HALO1, I3HALO2) sets to zero reads as zero.
 // Reads touch inner points only and writes touch halo points only, so one launch is safe.
 // Valid when every used axis has at least halo + 2 inner points (checked by the caller).
-template <typename S>
-__global__ void k_bc_halos(S* __restrict__ u, BcArgs a)
+//
+// Block partition (kBcThreads threads per block, every index decoded once per block):
+//   [0, nbx)            x faces: 16 rows (i2, i3) per block, 16 lanes per row = (side, k)
+//   [nbx, nbx+nby)      y faces: one run of up to kBcThreads i1 values per (i3, side, k)
+//   [nbx+nby, +nbz)     z faces: one run of up to kBcThreads i1 values per (i2, side, k)
+constexpr int kBcThreads = 256;
+
+struct BcPart {
+	int nbx, nby, nbz;     // blocks per group
+	int nchunk;            // i1 runs per row for y/z groups
+};
+
+BcPart bc_partition(const BcArgs& a, bool planes)
 {
-	const int axis = blockIdx.y;            // face pair along this axis
-	if (axis >= a.dim) return;
-	const int64_t nx = a.e[0] - a.s[0] + 1, ny = a.e[1] - a.s[1] + 1, nz = a.e[2] - a.s[2] + 1;
+	const int nx = (int)(a.e[0] - a.s[0] + 1), ny = (int)(a.e[1] - a.s[1] + 1),
+	          nz = (int)(a.e[2] - a.s[2] + 1);
+	const int kk = planes ? 1 : a.halo;     // planes: only k = 0 (the boundary plane itself)
+	BcPart p;
+	p.nchunk = (nx + kBcThreads - 1) / kBcThreads;
+	const int rows_per_block = kBcThreads / 16;
+	p.nbx = (ny * nz + rows_per_block - 1) / rows_per_block;
+	p.nby = a.dim >= 2 ? p.nchunk * nz * 2 * kk : 0;
+	p.nbz = a.dim >= 3 ? p.nchunk * ny * 2 * kk : 0;
+	return p;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kBcThreads) k_bc_halos(S* __restrict__ u, BcArgs a, BcPart p)
+{
 	const int R = a.halo;
-	// positions enumerated: (side, k, other axes) with the fastest index along i1 when possible
-	int64_t count;
-	if (axis == 0) count = 2 * (int64_t)R * ny * nz;
-	else if (axis == 1) count = 2 * (int64_t)R * nx * nz;
-	else count = 2 * (int64_t)R * nx * ny;
+	const int ny = (int)(a.e[1] - a.s[1] + 1);
 	const bool lo_x = a.faces & 1, hi_x = a.faces & 2, lo_y = a.faces & 4, hi_y = a.faces & 8;
-	for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
-			t += (int64_t)gridDim.x * blockDim.x) {
-		int64_t i1, i2, i3, m1, m2, m3;
-		bool zero = false;
-		if (axis == 0) {
-			const int k = (int)(t % R) + 1;
-			int64_t r = t / R;
-			const int side = (int)(r % 2);
-			r /= 2;
-			if (!(a.faces & (1 << side))) continue;
-			i2 = a.s[1] + r % ny;
-			i3 = a.s[2] + r / ny;
-			i1 = side ? a.e[0] + k : a.s[0] - k;
-			m1 = side ? a.e[0] - k : a.s[0] + k;
-			m2 = i2;
-			m3 = i3;
-		} else if (axis == 1) {
-			const int64_t x = t % nx;
-			int64_t r = t / nx;
-			const int k = (int)(r % R) + 1;
-			r /= R;
-			const int side = (int)(r % 2);
-			r /= 2;
-			if (!(a.faces & (4 << side))) continue;
-			i1 = a.s[0] + x;
-			i3 = a.s[2] + r;
-			i2 = side ? a.e[1] + k : a.s[1] - k;
-			m1 = i1;
-			m2 = side ? a.e[1] - k : a.s[1] + k;
-			m3 = i3;
-			zero = (lo_x && m1 == a.s[0]) || (hi_x && m1 == a.e[0]);
-		} else {
-			const int64_t x = t % nx;
-			int64_t r = t / nx;
-			const int64_t y = r % ny;
-			r /= ny;
-			const int k = (int)(r % R) + 1;
-			r /= R;
-			const int side = (int)r;
-			if (!(a.faces & (16 << side))) continue;
-			i1 = a.s[0] + x;
-			i2 = a.s[1] + y;
-			i3 = side ? a.e[2] + k : a.s[2] - k;
-			m1 = i1;
-			m2 = i2;
-			m3 = side ? a.e[2] - k : a.s[2] + k;
-			zero = (lo_x && m1 == a.s[0]) || (hi_x && m1 == a.e[0]) || (lo_y && m2 == a.s[1]) ||
-			       (hi_y && m2 == a.e[1]);
-		}
-		const S mv = zero ? S(0.0f) : u[m1 + m2 * a.n1 + m3 * a.n12];
-		u[i1 + i2 * a.n1 + i3 * a.n12] = Storage<S>::store(-Storage<S>::load(mv));
+	int b = blockIdx.x;
+	if (b < p.nbx) {
+		const int lane = threadIdx.x & 15;
+		if (lane >= 2 * R) return;
+		const int side = lane / R, k = lane % R + 1;
+		if (!(a.faces & (1 << side))) return;
+		const int row = b * (kBcThreads / 16) + (threadIdx.x >> 4);
+		const int nrow = ny * (int)(a.e[2] - a.s[2] + 1);
+		if (row >= nrow) return;
+		const int64_t base = (a.s[1] + row % ny) * a.n1 + (a.s[2] + row / ny) * a.n12;
+		const int64_t h = side ? a.e[0] + k : a.s[0] - k, m = side ? a.e[0] - k : a.s[0] + k;
+		u[base + h] = Storage<S>::store(-Storage<S>::load(u[base + m]));
+		return;
+	}
+	b -= p.nbx;
+	const int axis = (b < p.nby) ? 1 : 2;
+	if (axis == 2) b -= p.nby;
+	const int chunk = b % p.nchunk;
+	int r = b / p.nchunk;
+	const int ks = r % (2 * R);
+	r /= 2 * R;                                  // i3 (y faces) or i2 (z faces), inner offset
+	const int side = ks / R, k = ks % R + 1;
+	const int x = chunk * kBcThreads + threadIdx.x;
+	if (a.s[0] + x > a.e[0]) return;
+	const int64_t i1 = a.s[0] + x;
+	if (axis == 1) {
+		if (!(a.faces & (4 << side))) return;
+		const int64_t i3 = a.s[2] + r;
+		const int64_t h = side ? a.e[1] + k : a.s[1] - k, m = side ? a.e[1] - k : a.s[1] + k;
+		const bool zero = (lo_x && i1 == a.s[0]) || (hi_x && i1 == a.e[0]);
+		const S mv = zero ? S(0.0f) : u[i1 + m * a.n1 + i3 * a.n12];
+		u[i1 + h * a.n1 + i3 * a.n12] = Storage<S>::store(-Storage<S>::load(mv));
+	} else {
+		if (!(a.faces & (16 << side))) return;
+		const int64_t i2 = a.s[1] + r;
+		const int64_t h = side ? a.e[2] + k : a.s[2] - k, m = side ? a.e[2] - k : a.s[2] + k;
+		const bool zero = (lo_x && i1 == a.s[0]) || (hi_x && i1 == a.e[0]) ||
+		                  (lo_y && i2 == a.s[1]) || (hi_y && i2 == a.e[1]);
+		const S mv = zero ? S(0.0f) : u[i1 + i2 * a.n1 + m * a.n12];
+		u[i1 + i2 * a.n1 + h * a.n12] = Storage<S>::store(-Storage<S>::load(mv));
 	}
 }
 
-// Phase B: the boundary planes (first/last inner point of each active face) set to zero.
+// Phase B: the boundary planes (first/last inner point of each active face) set to zero,
+// same block partition with k = 0.
 template <typename S>
-__global__ void k_bc_planes(S* __restrict__ u, BcArgs a)
+__global__ void __launch_bounds__(kBcThreads) k_bc_planes(S* __restrict__ u, BcArgs a, BcPart p)
 {
-	const int axis = blockIdx.y;
-	if (axis >= a.dim) return;
-	const int64_t nx = a.e[0] - a.s[0] + 1, ny = a.e[1] - a.s[1] + 1, nz = a.e[2] - a.s[2] + 1;
-	int64_t count = (axis == 0) ? 2 * ny * nz : (axis == 1) ? 2 * nx * nz : 2 * nx * ny;
-	for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
-			t += (int64_t)gridDim.x * blockDim.x) {
-		int64_t i1, i2, i3;
-		if (axis == 0) {
-			const int side = (int)(t % 2);
-			const int64_t r = t / 2;
-			if (!(a.faces & (1 << side))) continue;
-			i1 = side ? a.e[0] : a.s[0];
-			i2 = a.s[1] + r % ny;
-			i3 = a.s[2] + r / ny;
-		} else if (axis == 1) {
-			const int64_t x = t % nx;
-			const int64_t r = t / nx;
-			const int side = (int)(r % 2);
-			if (!(a.faces & (4 << side))) continue;
-			i1 = a.s[0] + x;
-			i2 = side ? a.e[1] : a.s[1];
-			i3 = a.s[2] + r / 2;
-		} else {
-			const int64_t x = t % nx;
-			const int64_t r = t / nx;
-			const int64_t y = r % ny;
-			const int side = (int)(r / ny);
-			if (!(a.faces & (16 << side))) continue;
-			i1 = a.s[0] + x;
-			i2 = a.s[1] + y;
-			i3 = side ? a.e[2] : a.s[2];
-		}
-		u[i1 + i2 * a.n1 + i3 * a.n12] = S(0.0f);
+	const int ny = (int)(a.e[1] - a.s[1] + 1);
+	int b = blockIdx.x;
+	if (b < p.nbx) {
+		const int lane = threadIdx.x & 15;
+		if (lane >= 2) return;
+		const int side = lane;
+		if (!(a.faces & (1 << side))) return;
+		const int row = b * (kBcThreads / 16) + (threadIdx.x >> 4);
+		const int nrow = ny * (int)(a.e[2] - a.s[2] + 1);
+		if (row >= nrow) return;
+		const int64_t base = (a.s[1] + row % ny) * a.n1 + (a.s[2] + row / ny) * a.n12;
+		u[base + (side ? a.e[0] : a.s[0])] = S(0.0f);
+		return;
+	}
+	b -= p.nbx;
+	const int axis = (b < p.nby) ? 1 : 2;
+	if (axis == 2) b -= p.nby;
+	const int chunk = b % p.nchunk;
+	int r = b / p.nchunk;
+	const int side = r % 2;
+	r /= 2;
+	const int x = chunk * kBcThreads + threadIdx.x;
+	if (a.s[0] + x > a.e[0]) return;
+	const int64_t i1 = a.s[0] + x;
+	if (axis == 1) {
+		if (!(a.faces & (4 << side))) return;
+		u[i1 + (side ? a.e[1] : a.s[1]) * a.n1 + (a.s[2] + r) * a.n12] = S(0.0f);
+	} else {
+		if (!(a.faces & (16 << side))) return;
+		u[i1 + (a.s[1] + r) * a.n1 + (side ? a.e[2] : a.s[2]) * a.n12] = S(0.0f);
 	}
 }
 
@@ -456,10 +462,31 @@ int apply_boundary(const b200_layout* lay, const b200_field& u, int bc_type, int
 			}
 			return B200_OK;
 		}
-		const int blocks = num_sms() * 4;
-		k_bc_halos<S><<<dim3(blocks, lay->dim), 256, 0, s>>>(p, a);
+		const BcPart ph = bc_partition(a, false), pp = bc_partition(a, true);
+		k_bc_halos<S><<<ph.nbx + ph.nby + ph.nbz, kBcThreads, 0, s>>>(p, a, ph);
 		if (int rc = check_launch("k_bc_halos")) return rc;
-		k_bc_planes<S><<<dim3(blocks, lay->dim), 256, 0, s>>>(p, a);
+		k_bc_planes<S><<<pp.nbx + pp.nby + pp.nbz, kBcThreads, 0, s>>>(p, a, pp);
+		return check_launch("k_bc_planes");
+	});
+}
+
+// The boundary planes of the anti-mirror condition alone (its phase B): after a fused
+// propagator step, prc's inner boundary points become zero as applyBoundaryCondition leaves them.
+int apply_boundary_planes(const b200_layout* lay, const b200_field& u, int faces, cudaStream_t s)
+{
+	BcArgs a;
+	a.n1 = lay->n1;
+	a.n12 = lay->n1 * lay->n2;
+	a.s[0] = lay->s1; a.s[1] = lay->s2; a.s[2] = lay->s3;
+	a.e[0] = lay->e1; a.e[1] = lay->e2; a.e[2] = lay->e3;
+	a.halo = lay->halo;
+	a.dim = lay->dim;
+	a.faces = faces & 0x3F;
+	if (a.faces == 0) return B200_OK;
+	return dispatch_dtype(u.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		const BcPart pp = bc_partition(a, true);
+		k_bc_planes<S><<<pp.nbx + pp.nby + pp.nbz, kBcThreads, 0, s>>>(static_cast<S*>(u.data), a, pp);
 		return check_launch("k_bc_planes");
 	});
 }

@@ -95,6 +95,24 @@ int host_staging(size_t bytes, void** ptr)
 	return B200_OK;
 }
 
+// The library's device-side error word (set by kernels that give up a bounded wait).
+__device__ unsigned int g_device_error;
+
+int device_error_word(unsigned int** ptr)
+{
+	int dev;
+	if (int rc = current_device(&dev)) return rc;
+	static unsigned int* cached[kMaxDevices] = {};
+	if (!cached[dev]) {
+		void* p = nullptr;
+		if (int rc = cuda_error(cudaGetSymbolAddress(&p, g_device_error), "cudaGetSymbolAddress"))
+			return rc;
+		cached[dev] = static_cast<unsigned int*>(p);
+	}
+	*ptr = cached[dev];
+	return B200_OK;
+}
+
 int num_sms()
 {
 	int dev = 0;
@@ -234,6 +252,20 @@ int b200_memset(void* dptr, int value, size_t bytes, void* stream)
 	if (bytes == 0) return B200_OK;
 	if (!dptr) return set_error(B200_ERR_ARG, "NULL pointer");
 	return cuda_error(cudaMemsetAsync(dptr, value, bytes, as_stream(stream)), "cudaMemsetAsync");
+}
+
+int b200_device_status(int* status, int clear)
+{
+	if (!status) return set_error(B200_ERR_ARG, "status is NULL");
+	unsigned int v = 0;
+	int rc = cuda_error(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(v)), "cudaMemcpyFromSymbol");
+	if (rc) return rc;
+	*status = (int)v;
+	if (clear && v) {
+		const unsigned int zero = 0;
+		rc = cuda_error(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(zero)), "cudaMemcpyToSymbol");
+	}
+	return rc;
 }
 
 int b200_stream_sync(void* stream)

@@ -145,6 +145,7 @@ int run_stencil(int mode, const b200_layout* lay, int order, const b200_field& i
 
 int apply_boundary(const b200_layout* lay, const b200_field& u, int bc_type, int faces,
 		cudaStream_t s);
+int apply_boundary_planes(const b200_layout* lay, const b200_field& u, int faces, cudaStream_t s);
 
 }  // namespace b200
 
@@ -190,6 +191,20 @@ int b200_propagate_step(const b200_layout* lay, int order, b200_field prn, b200_
 {
 	if (int rc = check_layout(lay)) return rc;
 	if (int rc = check_field(prc, "prc")) return rc;
+	if (bc_type == B200_BOUND_COND_ANTI_MIRROR) {
+		// one kernel: the boundary condition of prc applied in the tiles of the pressure update
+		if (int rc = check_order(order)) return rc;
+		if (lay->halo != order / 2)
+			return set_error(B200_ERR_ARG, "layout halo %d does not match order %d", lay->halo, order);
+		if (int rc = check_field(prn, "prn")) return rc;
+		if (int rc = check_field(coef, "coef")) return rc;
+		if (int rc = check_same_grid(prc, prn, "propagate_step")) return rc;
+		int handled = 0;
+		if (int rc = run_zmarch(MODE_STEP, lay, order, prc, prn, &coef, inv2_1, inv2_2, inv2_3,
+					as_stream(stream), &handled))
+			return rc;
+		if (handled) return apply_boundary_planes(lay, prc, 0x3F, as_stream(stream));
+	}
 	if (int rc = apply_boundary(lay, prc, bc_type, 0x3F, as_stream(stream))) return rc;
 	return run_stencil(MODE_PRESSURE, lay, order, prc, prn, &coef, inv2_1, inv2_2, inv2_3,
 			as_stream(stream));

@@ -1,403 +1,26 @@
-// 3-D z-marching stencil kernels for sm_100a: FD_D2_N1/N2/N3, FD_LAPLACIAN and
-// computePressureWithFD (reference src/grid.cpp:3232-5113; the reference's best GPU form
-// of the same idea is src/grid_Cuda_Optim.cu:1085-2160, plain SIMT with a __shared__ tile
-// and per-plane __syncthreads).
+// Dispatcher, tensor maps, tuning table and autotuner of the 3-D z-marching stencil
+// kernels (the kernel itself is in b200_zmarch.cuh).
 //
-// Design (one CTA = one TX x TY tile of (i1, i2) marching over a chunk of i3 planes):
-//  * a producer warp streams the planes of the input grid into a ring of shared-memory
-//    tiles with TMA (cp.async.bulk.tensor.3d, no cluster multicast): plane tile with the
-//    x/y halos the operator needs, plus, for the pressure update, the prn and coef tiles
-//    of the output plane. Full/empty mbarriers hand the slots between producer and
-//    consumers; the ring runs PF planes ahead of the consumers;
-//  * consumer threads own VX consecutive i1 points (16 bytes, one vector shared-memory
-//    load) of VY consecutive rows and keep the 2R+1 values of each point along i3 in a
-//    register queue, so every plane is read from HBM once (plus the chunk's z-halo);
-//  * the x/y derivatives read the staged tile of the centre plane, which the ring keeps
-//    resident for R iterations after it arrives;
-//  * every operation is a separately rounded IEEE operation in the reference's order,
-//    so the results are bit-identical to the reference CPU path.
-// Every wait on an mbarrier is bounded by a time limit: a CTA that gives up records an
-// error flag (read by b200_device_status) and returns after its issued copies have landed.
-#include <cuda.h>
+// Tuning: for every (storage type, order, operator) the launch uses a tile shape and a
+// number of planes per CTA. Defaults come from a heuristic; b200_autotune_stencil times
+// every shape and chunk candidate on scratch grids of the caller's layout and records the
+// fastest, which every later launch of that key uses (the reference's -cb1/-cb2/-cb3
+// cache-block sweep, src/grid_Cuda_Optim.cu:2163-2211 and script/testCase_FD_D2/
+// cacheBlkAnalysis, made automatic).
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
 
-#include <cstring>
-
-#include "b200_stencil.cuh"
+#include "b200_zmarch.cuh"
 
 namespace b200 {
 
-__device__ unsigned int g_device_error;
+int apply_boundary(const b200_layout* lay, const b200_field& u, int bc_type, int faces,
+		cudaStream_t s);
 
 namespace {
 
-// ---- PTX wrappers -------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-	return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-			: "memory");
-}
-
-__device__ __forceinline__ void fence_mbar_init()
-{
-	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-			"r"(bytes)
-			: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-	uint32_t ok;
-	asm volatile(
-			"{\n\t.reg .pred p;\n\t"
-			"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-			"selp.u32 %0, 1, 0, p;\n\t}"
-			: "=r"(ok)
-			: "r"(smem_u32(bar)), "r"(parity)
-			: "memory");
-	return ok != 0;
-}
-
-__device__ __forceinline__ uint64_t global_timer_ns()
-{
-	uint64_t t;
-	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-	return t;
-}
-
-// Wait for the completion of the mbarrier phase of the given parity, at most until
-// `deadline` (global timer, ns). Returns false when the time ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t deadline)
-{
-	if (mbar_try_wait(bar, parity)) return true;
-	for (uint32_t n = 1;; ++n) {
-		if (mbar_try_wait(bar, parity)) return true;
-		if ((n & 63u) == 0 && global_timer_ns() > deadline) return false;
-	}
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, int x, int y, int z,
-		uint64_t* bar)
-{
-	asm volatile(
-			"cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-			" [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-			"l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-			: "memory");
-}
-
-__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* tm)
-{
-	asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");
-}
-
-// ---- vector shared-memory loads (16 bytes) converted to the compute type --------------------------
-template <typename S, typename C, int N>
-__device__ __forceinline__ void lds_vec(const S* p, C* out)
-{
-	static_assert(N * sizeof(S) % 16 == 0, "vector of 16-byte multiples");
-#pragma unroll
-	for (int b = 0; b < N * (int)sizeof(S) / 16; b++) {
-		const uint4 raw = reinterpret_cast<const uint4*>(p)[b];
-		const S* v = reinterpret_cast<const S*>(&raw);
-#pragma unroll
-		for (int i = 0; i < 16 / (int)sizeof(S); i++)
-			out[b * (16 / sizeof(S)) + i] = Storage<S>::load(v[i]);
-	}
-}
-
-constexpr int round_up(int v, int m) { return (v + m - 1) / m * m; }
-
-// ---- kernel configuration -----------------------------------------------------------------------
-template <typename S, int R_, int MODE_, int TX_, int TY_, int VY_, int PF_>
-struct ZCfg {
-	using Stor = S;
-	using C = typename Storage<S>::C;
-	static constexpr int R = R_;
-	static constexpr int MODE = MODE_;
-	static constexpr int TX = TX_, TY = TY_, VY = VY_, PF = PF_;
-	static constexpr int VX = 16 / sizeof(S);
-	static constexpr bool XH = (MODE == MODE_D2_AXIS1 || MODE == MODE_LAPLACIAN || MODE == MODE_PRESSURE);
-	static constexpr bool YH = (MODE == MODE_D2_AXIS2 || MODE == MODE_LAPLACIAN || MODE == MODE_PRESSURE);
-	static constexpr bool ZQ = (MODE == MODE_D2_AXIS3 || MODE == MODE_LAPLACIAN || MODE == MODE_PRESSURE);
-	static constexpr bool P = (MODE == MODE_PRESSURE);
-	static constexpr int R4 = XH ? round_up(R, VX) : 0;     // x halo, whole vectors
-	static constexpr int RY = YH ? R : 0;
-	static constexpr int RZ = ZQ ? R : 0;
-	static constexpr int BX = TX + 2 * R4;
-	static constexpr int BY = TY + 2 * RY;
-	static constexpr int NSU = RZ + 1 + PF;                  // input-tile ring
-	static constexpr int NSP = P ? 1 + PF : 1;               // prn/coef ring
-	static constexpr int U_BYTES = BX * BY * (int)sizeof(S);
-	static constexpr int U_STRIDE = round_up(U_BYTES, 128);
-	static constexpr int PT_BYTES = TX * TY * (int)sizeof(S);
-	static constexpr int PT_STRIDE = round_up(PT_BYTES, 128);
-	static constexpr int NTX = TX / VX;
-	static constexpr int NC = NTX * (TY / VY);              // consumer threads
-	static constexpr int NWC = NC / 32;                      // consumer warps
-	static constexpr int NT = NC + 32;                       // + one producer warp
-	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * 2 * PT_STRIDE : 0) +
-	                            (2 * NSU + 2 * NSP) * 8;
-	static_assert(TX % VX == 0 && TY % VY == 0 && NC % 32 == 0, "tile shape");
-	static_assert(BX <= 256 && BY <= 256, "TMA box limit");
-	static_assert((BX * sizeof(S)) % 16 == 0 && (TX * sizeof(S)) % 16 == 0, "TMA inner extent");
-};
-
-template <typename C>
-struct ZArgs {
-	void* out;                 // w, or prn for the pressure update
-	int64_t n1, n12;
-	int x_start;               // first tile's i1 (16-byte aligned index)
-	int s1, e1, s2, e2, s3, e3;
-	int nz_chunk;
-	C inv2_1, inv2_2, inv2_3;
-	float coef_scale;
-	uint64_t timeout_ns;
-};
-
-
-template <class Cfg>
-__global__ void __launch_bounds__(Cfg::NT) k_zmarch(const __grid_constant__ CUtensorMap tm_u,
-		const __grid_constant__ CUtensorMap tm_prn, const __grid_constant__ CUtensorMap tm_coef,
-		const ZArgs<typename Cfg::C> a)
-{
-	using S = typename Cfg::Stor;
-	using C = typename Cfg::C;
-	using A = Arith<true>;
-	constexpr int R = Cfg::R, VX = Cfg::VX, VY = Cfg::VY, TX = Cfg::TX;
-	constexpr int R4 = Cfg::R4, RY = Cfg::RY, RZ = Cfg::RZ, BX = Cfg::BX;
-	constexpr int NSU = Cfg::NSU, NSP = Cfg::NSP, NC = Cfg::NC;
-	constexpr int UE = Cfg::U_STRIDE / (int)sizeof(S);     // elements between input tiles
-	constexpr int PE = Cfg::PT_STRIDE / (int)sizeof(S);    // elements between prn/coef tiles
-	constexpr unsigned FULL = 0xffffffffu;
-
-	extern __shared__ unsigned char smem_raw[];
-	unsigned char* smem = reinterpret_cast<unsigned char*>(
-			(reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-	S* su = reinterpret_cast<S*>(smem);
-	S* sp = reinterpret_cast<S*>(smem + NSU * Cfg::U_STRIDE);
-	uint64_t* bars = reinterpret_cast<uint64_t*>(
-			smem + NSU * Cfg::U_STRIDE + (Cfg::P ? NSP * 2 * Cfg::PT_STRIDE : 0));
-	uint64_t* full_u = bars;
-	uint64_t* empty_u = bars + NSU;
-	uint64_t* full_p = bars + 2 * NSU;
-	uint64_t* empty_p = full_p + NSP;
-
-	const int tile_x0 = a.x_start + (int)blockIdx.x * TX;
-	const int tile_y0 = a.s2 + (int)blockIdx.y * Cfg::TY;
-	const int z0 = a.s3 + (int)blockIdx.z * a.nz_chunk;
-	const int z1 = min(z0 + a.nz_chunk, a.e3 + 1);
-	const int J = (z1 - z0) + 2 * RZ;          // planes this CTA streams in
-
-	if (threadIdx.x == 0) {
-		for (int s = 0; s < NSU; s++) {
-			mbar_init(&full_u[s], 1);
-			mbar_init(&empty_u[s], Cfg::NWC);
-		}
-		for (int s = 0; s < NSP; s++) {
-			mbar_init(&full_p[s], 1);
-			mbar_init(&empty_p[s], Cfg::NWC);
-		}
-		fence_mbar_init();
-	}
-	__syncthreads();
-	const uint64_t deadline = global_timer_ns() + a.timeout_ns;
-
-	if (threadIdx.x >= NC) {
-		// ---- producer: one thread issues every TMA copy ------------------------------------------
-		if (threadIdx.x != NC) return;
-		prefetch_tmap(&tm_u);
-		if constexpr (Cfg::P) {
-			prefetch_tmap(&tm_prn);
-			prefetch_tmap(&tm_coef);
-		}
-		int issued_u = 0, issued_p = 0;
-		bool ok = true;
-		for (int j = 0; j < J; ++j) {
-			const int s = j % NSU;
-			if (j >= NSU && !mbar_wait(&empty_u[s], ((j / NSU) - 1) & 1, deadline)) {
-				ok = false;
-				break;
-			}
-			mbar_arrive_expect_tx(&full_u[s], Cfg::U_BYTES);
-			tma_load_3d(su + s * UE, &tm_u, tile_x0 - R4, tile_y0 - RY, z0 - RZ + j, &full_u[s]);
-			issued_u = j + 1;
-			if constexpr (Cfg::P) {
-				if (j >= 2 * RZ) {
-					const int o = j - 2 * RZ, t = o % NSP;
-					if (o >= NSP && !mbar_wait(&empty_p[t], ((o / NSP) - 1) & 1, deadline)) {
-						ok = false;
-						break;
-					}
-					mbar_arrive_expect_tx(&full_p[t], 2 * Cfg::PT_BYTES);
-					tma_load_3d(sp + (2 * t) * PE, &tm_prn, tile_x0, tile_y0, z0 + o, &full_p[t]);
-					tma_load_3d(sp + (2 * t + 1) * PE, &tm_coef, tile_x0, tile_y0, z0 + o, &full_p[t]);
-					issued_p = o + 1;
-				}
-			}
-		}
-		if (!ok) atomicOr(&g_device_error, 1u);
-		// every issued copy lands before the CTA may retire its shared memory
-		const uint64_t drain = global_timer_ns() + a.timeout_ns;
-		for (int j = max(0, issued_u - NSU); j < issued_u; ++j)
-			mbar_wait(&full_u[j % NSU], (j / NSU) & 1, drain);
-		for (int o = max(0, issued_p - NSP); o < issued_p; ++o)
-			mbar_wait(&full_p[o % NSP], (o / NSP) & 1, drain);
-		return;
-	}
-
-	// ---- consumers ---------------------------------------------------------------------------
-	const int tid = threadIdx.x;
-	const int lane = tid & 31;
-	const int xl = (tid % Cfg::NTX) * VX;
-	const int yl = (tid / Cfg::NTX) * VY;
-	C q[2 * RZ + 1][VY][VX];           // values along i3 of this thread's points
-	bool ok = true;
-	for (int j = 0; j < J; ++j) {
-		const int s = j % NSU;
-		if (!__all_sync(FULL, mbar_wait(&full_u[s], (j / NSU) & 1, deadline))) {
-			ok = false;
-			break;
-		}
-		if constexpr (Cfg::ZQ) {
-#pragma unroll
-			for (int i = 0; i < 2 * RZ; i++)
-#pragma unroll
-				for (int v = 0; v < VY; v++)
-#pragma unroll
-					for (int e = 0; e < VX; e++) q[i][v][e] = q[i + 1][v][e];
-			const S* t = su + s * UE;
-#pragma unroll
-			for (int v = 0; v < VY; v++) lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl, q[2 * RZ][v]);
-		}
-		if (j >= 2 * RZ) {
-			const int o = j - 2 * RZ;
-			const int k = z0 + o;                     // output plane
-			const int sc = (j - RZ) % NSU;            // slot holding plane k with its halos
-			const S* t = su + sc * UE;
-			const S* pt = nullptr;
-			if constexpr (Cfg::P) {
-				const int tp = o % NSP;
-				if (!__all_sync(FULL, mbar_wait(&full_p[tp], (o / NSP) & 1, deadline))) {
-					ok = false;
-					break;
-				}
-				pt = sp + (2 * tp) * PE;
-			}
-			// rows of this thread's columns, plane k: (VY + 2 RY) x VX values
-			C yv[VY + 2 * RY][VX];
-#pragma unroll
-			for (int r = 0; r < VY + 2 * RY; r++) {
-				const int v = r - RY;
-				if (v >= 0 && v < VY && Cfg::ZQ) {
-#pragma unroll
-					for (int e = 0; e < VX; e++) yv[r][e] = q[RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
-				} else {
-					lds_vec<S, C, VX>(t + (yl + r) * BX + R4 + xl, yv[r]);
-				}
-			}
-			const int Y0 = tile_y0 + yl;
-			const int X = tile_x0 + xl;
-#pragma unroll
-			for (int v = 0; v < VY; v++) {
-				C res[VX];
-				C dx[VX], dy[VX], dz[VX];
-				if constexpr (Cfg::XH) {
-					C xv[VX + 2 * R4];
-#pragma unroll
-					for (int h = 0; h < R4 / VX; h++)
-						lds_vec<S, C, VX>(t + (yl + v + RY) * BX + xl + h * VX, &xv[h * VX]);
-#pragma unroll
-					for (int e = 0; e < VX; e++) xv[R4 + e] = yv[v + RY][e];
-#pragma unroll
-					for (int h = 0; h < R4 / VX; h++)
-						lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl + VX + h * VX,
-								&xv[R4 + VX + h * VX]);
-#pragma unroll
-					for (int e = 0; e < VX; e++)
-						dx[e] = d2_axis<C, R, true>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
-				}
-				if constexpr (Cfg::YH) {
-#pragma unroll
-					for (int e = 0; e < VX; e++)
-						dy[e] = d2_axis<C, R, true>([&](int kk) { return yv[v + RY + kk][e]; }, a.inv2_2);
-				}
-				if constexpr (Cfg::ZQ) {
-#pragma unroll
-					for (int e = 0; e < VX; e++)
-						dz[e] = d2_axis<C, R, true>([&](int kk) { return q[RZ + kk][v][e]; }, a.inv2_3);
-				}
-				if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
-#pragma unroll
-					for (int e = 0; e < VX; e++) res[e] = dx[e];
-				} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
-#pragma unroll
-					for (int e = 0; e < VX; e++) res[e] = dy[e];
-				} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
-#pragma unroll
-					for (int e = 0; e < VX; e++) res[e] = dz[e];
-				} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
-#pragma unroll
-					for (int e = 0; e < VX; e++) res[e] = A::add(A::add(dx[e], dy[e]), dz[e]);
-				} else {
-					C pn[VX], cf[VX];
-					lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
-					lds_vec<S, C, VX>(pt + PE + (yl + v) * TX + xl, cf);
-#pragma unroll
-					for (int e = 0; e < VX; e++) {
-						C c = cf[e];
-						if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
-						res[e] = leapfrog<C, true>(yv[v + RY][e], pn[e], c,
-								A::add(A::add(dx[e], dy[e]), dz[e]));
-					}
-				}
-				const int Y = Y0 + v;
-				if (Y <= a.e2) {
-					S* dst = static_cast<S*>(a.out) + X + (int64_t)Y * a.n1 + (int64_t)k * a.n12;
-					if (X >= a.s1 && X + VX - 1 <= a.e1) {
-						uint4 pk;
-						S* ps = reinterpret_cast<S*>(&pk);
-#pragma unroll
-						for (int e = 0; e < VX; e++) ps[e] = Storage<S>::store(res[e]);
-						*reinterpret_cast<uint4*>(dst) = pk;
-					} else {
-#pragma unroll
-						for (int e = 0; e < VX; e++)
-							if (X + e >= a.s1 && X + e <= a.e1) dst[e] = Storage<S>::store(res[e]);
-					}
-				}
-			}
-			__syncwarp();
-			if (lane == 0) {
-				mbar_arrive(&empty_u[sc]);
-				if constexpr (Cfg::P) mbar_arrive(&empty_p[o % NSP]);
-			}
-		}
-		if constexpr (Cfg::ZQ) {
-			if (j < RZ || j >= J - RZ) {   // planes that are never a centre plane
-				__syncwarp();
-				if (lane == 0) mbar_arrive(&empty_u[s]);
-			}
-		}
-	}
-	if (!ok && lane == 0) atomicOr(&g_device_error, 2u);
-}
-
-// ---- host side ------------------------------------------------------------------------------------
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
 		const cuuint64_t*, const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
 		CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -429,6 +52,57 @@ CUtensorMapDataType tma_dtype(int dtype)
 	}
 }
 
+bool has_shapes(int mode)
+{
+	return mode == MODE_PRESSURE || mode == MODE_LAPLACIAN || mode == MODE_STEP;
+}
+
+// ---- tuning table --------------------------------------------------------------------------
+struct Tuned {
+	int shape = 0;
+	int nz_chunk = 0;   // 0: heuristic
+	bool fused = false; // MODE_STEP only: the fused kernel beat BC + pressure when tuned
+};
+using TuneKey = std::tuple<int, int, int, int>;   // dtype, R, mode, exact
+std::map<TuneKey, Tuned> g_tuned;
+std::mutex g_tune_mutex;
+int g_arith = B200_ARITH_EXACT;
+
+// Untuned defaults: the fastest shape measured at 512^3 on B200 for each storage type and
+// half width (FP32: two-row 28x64 tiles up to R = 2, 9-warp 16x64 tiles for R = 3..4,
+// 30x64 tiles with 128-plane chunks beyond; FP64: 14x32 tiles up to R = 4).
+Tuned default_tuning(int dtype, int R)
+{
+	Tuned t;
+	if (dtype == B200_F64) {
+		t.shape = R <= 4 ? 0 : 1;
+	} else {
+		t.shape = R <= 2 ? 0 : (R <= 4 ? 2 : 1);
+	}
+	t.nz_chunk = R > 4 ? 128 : 0;
+	return t;
+}
+
+Tuned tuned_for(int dtype, int R, int mode, bool exact)
+{
+	std::lock_guard<std::mutex> lock(g_tune_mutex);
+	auto it = g_tuned.find(TuneKey{dtype, R, mode, exact ? 1 : 0});
+	if (it != g_tuned.end()) return it->second;
+	return has_shapes(mode) ? default_tuning(dtype, R) : Tuned{};
+}
+
+int launch(const ZLaunch& L)
+{
+	switch (L.mode) {
+	case MODE_STEP: return zmarch_launch_step(L);
+	case MODE_PRESSURE: return zmarch_launch_pressure(L);
+	case MODE_LAPLACIAN: return zmarch_launch_laplacian(L);
+	default: return zmarch_launch_d2(L);
+	}
+}
+
+}  // namespace
+
 int make_map(CUtensorMap* m, const void* base, int dtype, const b200_layout* lay, int bx, int by)
 {
 	EncodeTiledFn enc;
@@ -447,72 +121,6 @@ int make_map(CUtensorMap* m, const void* base, int dtype, const b200_layout* lay
 	return B200_OK;
 }
 
-// planes per CTA: enough CTAs for several waves, long enough chunks to amortise the z-halo
-template <class Cfg>
-int pick_nz_chunk(int ntiles, int nz)
-{
-	int per_sm = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zmarch<Cfg>, Cfg::NT, Cfg::SMEM);
-	if (per_sm < 1) per_sm = 1;
-	const int resident = per_sm * num_sms();
-	int chunk = 64;
-	while (chunk > 16 && (int64_t)ntiles * ((nz + chunk - 1) / chunk) < 4 * (int64_t)resident) chunk /= 2;
-	return chunk < nz ? chunk : nz;
-}
-
-template <class Cfg>
-int launch_zmarch(const b200_layout* lay, const b200_field& in, const b200_field& out,
-		const b200_field* coef, double inv2_1, double inv2_2, double inv2_3, cudaStream_t s)
-{
-	using C = typename Cfg::C;
-	int rc = cuda_error(cudaFuncSetAttribute(k_zmarch<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                            Cfg::SMEM), "cudaFuncSetAttribute(k_zmarch)");
-	if (rc) return rc;
-	alignas(64) CUtensorMap tm_u, tm_p, tm_c;
-	if ((rc = make_map(&tm_u, in.data, in.dtype, lay, Cfg::BX, Cfg::BY))) return rc;
-	if (Cfg::P) {
-		if ((rc = make_map(&tm_p, out.data, out.dtype, lay, Cfg::TX, Cfg::TY))) return rc;
-		if ((rc = make_map(&tm_c, coef->data, coef->dtype, lay, Cfg::TX, Cfg::TY))) return rc;
-	} else {
-		tm_p = tm_u;
-		tm_c = tm_u;
-	}
-	ZArgs<C> a;
-	a.out = out.data;
-	a.n1 = lay->n1;
-	a.n12 = lay->n1 * lay->n2;
-	a.x_start = (int)(lay->s1 / Cfg::VX) * Cfg::VX;
-	a.s1 = (int)lay->s1; a.e1 = (int)lay->e1;
-	a.s2 = (int)lay->s2; a.e2 = (int)lay->e2;
-	a.s3 = (int)lay->s3; a.e3 = (int)lay->e3;
-	a.inv2_1 = (C)inv2_1;
-	a.inv2_2 = (C)inv2_2;
-	a.inv2_3 = (C)inv2_3;
-	a.coef_scale = coef ? coef->scale : 1.0f;
-	a.timeout_ns = 2000000000ull;
-	const int ntx = (a.e1 + 1 - a.x_start + Cfg::TX - 1) / Cfg::TX;
-	const int nty = (a.e2 - a.s2 + 1 + Cfg::TY - 1) / Cfg::TY;
-	const int nz = a.e3 - a.s3 + 1;
-	a.nz_chunk = pick_nz_chunk<Cfg>(ntx * nty, nz);
-	const int nzc = (nz + a.nz_chunk - 1) / a.nz_chunk;
-	k_zmarch<Cfg><<<dim3(ntx, nty, nzc), Cfg::NT, Cfg::SMEM, s>>>(tm_u, tm_p, tm_c, a);
-	return check_launch("k_zmarch");
-}
-
-// tile shapes per storage type and half width
-template <typename S, int R, int MODE>
-int launch_for(const b200_layout* lay, const b200_field& in, const b200_field& out,
-		const b200_field* coef, double i1, double i2, double i3, cudaStream_t s)
-{
-	if constexpr (sizeof(S) == 8) {
-		return launch_zmarch<ZCfg<S, R, MODE, 32, 16, 1, 2>>(lay, in, out, coef, i1, i2, i3, s);
-	} else {
-		return launch_zmarch<ZCfg<S, R, MODE, 64, 16, 1, 2>>(lay, in, out, coef, i1, i2, i3, s);
-	}
-}
-
-}  // namespace
-
 bool zmarch_accepts(const b200_layout* lay, int dtype)
 {
 	if (lay->dim != 3) return false;
@@ -528,42 +136,187 @@ int run_zmarch(int mode, const b200_layout* lay, int order, const b200_field& in
 {
 	*handled = 0;
 	if (!zmarch_accepts(lay, in.dtype)) return B200_OK;
+	if (mode == MODE_STEP) {
+		// the in-tile boundary condition needs mirror points that are never boundary points
+		if (lay->e1 - lay->s1 + 1 < lay->halo + 2 || lay->e2 - lay->s2 + 1 < lay->halo + 2 ||
+				lay->e3 - lay->s3 + 1 < lay->halo + 2)
+			return B200_OK;
+	}
 	if ((reinterpret_cast<uintptr_t>(in.data) | reinterpret_cast<uintptr_t>(out.data)) % 16) return B200_OK;
 	if (coef) {
 		if (coef->dtype != in.dtype) return B200_OK;
 		if (reinterpret_cast<uintptr_t>(coef->data) % 16) return B200_OK;
 	}
+	const bool exact = !has_shapes(mode) || g_arith == B200_ARITH_EXACT;
+	const Tuned t = tuned_for(in.dtype, order / 2, mode, exact);
+	if (mode == MODE_STEP && !t.fused) return B200_OK;   // separate BC + pressure is faster
 	*handled = 1;
-	return dispatch_order(order, [&](auto rt) {
-		constexpr int R = decltype(rt)::value;
-		auto go = [&](auto tag) {
-			using S = decltype(tag);
-			switch (mode) {
-			case MODE_D2_AXIS1: return launch_for<S, R, MODE_D2_AXIS1>(lay, in, out, coef, inv2_1, inv2_2, inv2_3, s);
-			case MODE_D2_AXIS2: return launch_for<S, R, MODE_D2_AXIS2>(lay, in, out, coef, inv2_1, inv2_2, inv2_3, s);
-			case MODE_D2_AXIS3: return launch_for<S, R, MODE_D2_AXIS3>(lay, in, out, coef, inv2_1, inv2_2, inv2_3, s);
-			case MODE_LAPLACIAN: return launch_for<S, R, MODE_LAPLACIAN>(lay, in, out, coef, inv2_1, inv2_2, inv2_3, s);
-			default: return launch_for<S, R, MODE_PRESSURE>(lay, in, out, coef, inv2_1, inv2_2, inv2_3, s);
-			}
-		};
-		if (in.dtype == B200_F64) return go(double{});
-		return go(float{});
-	});
+	ZLaunch L;
+	L.mode = mode;
+	L.lay = lay;
+	L.R = order / 2;
+	L.in = &in;
+	L.out = &out;
+	L.coef = coef;
+	L.inv2[0] = inv2_1;
+	L.inv2[1] = inv2_2;
+	L.inv2[2] = inv2_3;
+	L.s = s;
+	L.exact = exact;
+	L.shape = t.shape;
+	L.nz_chunk = t.nz_chunk;
+	if (int rc = device_error_word(&L.err)) return rc;
+	return launch(L);
 }
 
 }  // namespace b200
 
-extern "C" int b200_device_status(int* status, int clear)
+using namespace b200;
+
+extern "C" {
+
+int b200_set_arith_mode(int mode)
 {
-	using namespace b200;
-	if (!status) return set_error(B200_ERR_ARG, "status is NULL");
-	unsigned int v = 0;
-	int rc = cuda_error(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(v)), "cudaMemcpyFromSymbol");
-	if (rc) return rc;
-	*status = (int)v;
-	if (clear && v) {
-		const unsigned int zero = 0;
-		rc = cuda_error(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(zero)), "cudaMemcpyToSymbol");
-	}
-	return rc;
+	if (mode != B200_ARITH_EXACT && mode != B200_ARITH_FMA)
+		return set_error(B200_ERR_ARG, "arithmetic mode %d", mode);
+	g_arith = mode;
+	return B200_OK;
 }
+
+int b200_get_arith_mode(int* mode)
+{
+	if (!mode) return set_error(B200_ERR_ARG, "mode is NULL");
+	*mode = g_arith;
+	return B200_OK;
+}
+
+int b200_set_stencil_config(int dtype, int order, int op, int shape, int nz_chunk)
+{
+	if (int rc = check_order(order)) return rc;
+	if (dtype != B200_F32 && dtype != B200_F64)
+		return set_error(B200_ERR_UNSUPPORTED, "tuned kernels exist for FP32 and FP64 only");
+	if (op < MODE_D2_AXIS1 || op > MODE_STEP) return set_error(B200_ERR_ARG, "operator %d", op);
+	if (shape < -1 || shape >= (has_shapes(op) ? kZShapes : 1))
+		return set_error(B200_ERR_ARG, "shape %d", shape);
+	if (nz_chunk < 0) return set_error(B200_ERR_ARG, "nz_chunk %d", nz_chunk);
+	std::lock_guard<std::mutex> lock(g_tune_mutex);
+	if (shape == -1) {   // back to the untuned defaults
+		for (int ex = 0; ex < 2; ex++) g_tuned.erase(TuneKey{dtype, order / 2, op, ex});
+		return B200_OK;
+	}
+	// setting a shape for the fused step selects the fused kernel
+	for (int ex = 0; ex < 2; ex++)
+		g_tuned[TuneKey{dtype, order / 2, op, ex}] = Tuned{shape, nz_chunk, op == MODE_STEP};
+	return B200_OK;
+}
+
+int b200_get_stencil_config(int dtype, int order, int op, int* shape, int* nz_chunk)
+{
+	if (!shape || !nz_chunk) return set_error(B200_ERR_ARG, "NULL output");
+	if (int rc = check_order(order)) return rc;
+	const Tuned t = tuned_for(dtype, order / 2, op, g_arith == B200_ARITH_EXACT || !has_shapes(op));
+	*shape = t.shape;
+	*nz_chunk = t.nz_chunk;
+	return B200_OK;
+}
+
+int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, int reps,
+		int* best_shape, int* best_chunk, double* best_ms)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_order(order)) return rc;
+	if (lay->halo != order / 2) return set_error(B200_ERR_ARG, "layout halo does not match order");
+	if (!zmarch_accepts(lay, dtype))
+		return set_error(B200_ERR_UNSUPPORTED, "layout/dtype not handled by the z-marching kernels");
+	if (op < MODE_D2_AXIS1 || op > MODE_STEP) return set_error(B200_ERR_ARG, "operator %d", op);
+	if (reps < 1) reps = 5;
+	const size_t bytes = (size_t)npoint(lay) * dtype_size(dtype);
+	void* buf[3] = {nullptr, nullptr, nullptr};
+	int rc = B200_OK;
+	for (int i = 0; i < 3 && !rc; i++) {
+		rc = cuda_error(cudaMalloc(&buf[i], bytes), "cudaMalloc(autotune)");
+		if (!rc) rc = cuda_error(cudaMemset(buf[i], 0, bytes), "cudaMemset(autotune)");
+	}
+	cudaStream_t s = nullptr;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	if (!rc) rc = cuda_error(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+	if (!rc) rc = cuda_error(cudaEventCreate(&e0), "cudaEventCreate");
+	if (!rc) rc = cuda_error(cudaEventCreate(&e1), "cudaEventCreate");
+	const b200_field fin{buf[0], dtype, 1.0f}, fout{buf[1], dtype, 1.0f}, fcoef{buf[2], dtype, 1.0f};
+	ZLaunch L;
+	L.mode = op;
+	L.lay = lay;
+	L.R = order / 2;
+	L.in = &fin;
+	L.out = &fout;
+	L.coef = (op == MODE_PRESSURE || op == MODE_STEP) ? &fcoef : nullptr;
+	L.inv2[0] = L.inv2[1] = L.inv2[2] = 1.0;
+	L.s = s;
+	L.exact = !has_shapes(op) || g_arith == B200_ARITH_EXACT;
+	if (!rc) rc = device_error_word(&L.err);
+	const int nz = (int)(lay->e3 - lay->s3 + 1);
+	const std::vector<int> chunks = {0, 16, 32, 64, 128};
+	double best = 1e300;
+	Tuned win{};
+	const int nshape = has_shapes(op) ? kZShapes : 1;
+	for (int sh = 0; sh < nshape && !rc; sh++) {
+		for (int c : chunks) {
+			if (c > nz) continue;
+			L.shape = sh;
+			L.nz_chunk = c;
+			if ((rc = launch(L))) break;      // warm-up (and first-use module load)
+			if ((rc = cuda_error(cudaEventRecord(e0, s), "cudaEventRecord"))) break;
+			for (int r = 0; r < reps && !rc; r++) rc = launch(L);
+			if (rc) break;
+			if ((rc = cuda_error(cudaEventRecord(e1, s), "cudaEventRecord"))) break;
+			if ((rc = cuda_error(cudaEventSynchronize(e1), "cudaEventSynchronize"))) break;
+			float ms = 0.f;
+			cudaEventElapsedTime(&ms, e0, e1);
+			ms /= reps;
+			if (ms < best) {
+				best = ms;
+				win = Tuned{sh, c};
+			}
+		}
+	}
+	if (!rc && op == MODE_STEP) {
+		// the alternative: the boundary condition kernels + the best pressure kernel
+		ZLaunch P = L;
+		P.mode = MODE_PRESSURE;
+		const Tuned tp = tuned_for(dtype, order / 2, MODE_PRESSURE, L.exact);
+		P.shape = tp.shape;
+		P.nz_chunk = tp.nz_chunk;
+		double sep = 1e300;
+		auto run_sep = [&]() {
+			int r = apply_boundary(lay, fin, B200_BOUND_COND_ANTI_MIRROR, 0x3F, s);
+			return r ? r : launch(P);
+		};
+		if (!(rc = run_sep()) && !(rc = cuda_error(cudaEventRecord(e0, s), "cudaEventRecord"))) {
+			for (int r = 0; r < reps && !rc; r++) rc = run_sep();
+			if (!rc && !(rc = cuda_error(cudaEventRecord(e1, s), "cudaEventRecord")) &&
+					!(rc = cuda_error(cudaEventSynchronize(e1), "cudaEventSynchronize"))) {
+				float ms = 0.f;
+				cudaEventElapsedTime(&ms, e0, e1);
+				sep = ms / reps;
+			}
+		}
+		win.fused = best < sep;
+		if (!win.fused) best = sep;
+	}
+	if (e0) cudaEventDestroy(e0);
+	if (e1) cudaEventDestroy(e1);
+	if (s) cudaStreamDestroy(s);
+	for (void* p : buf)
+		if (p) cudaFree(p);
+	if (rc) return rc;
+	{
+		std::lock_guard<std::mutex> lock(g_tune_mutex);
+		g_tuned[TuneKey{dtype, order / 2, op, L.exact ? 1 : 0}] = win;
+	}
+	if (best_shape) *best_shape = (op == MODE_STEP && !win.fused) ? -1 : win.shape;
+	if (best_chunk) *best_chunk = win.nz_chunk;
+	if (best_ms) *best_ms = best;
+	return B200_OK;
+}
+
+}  // extern "C"

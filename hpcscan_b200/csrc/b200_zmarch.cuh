@@ -1,0 +1,702 @@
+// 3-D z-marching stencil kernels for sm_100a: FD_D2_N1/N2/N3, FD_LAPLACIAN and
+// computePressureWithFD (reference src/grid.cpp:3232-5113; the reference's best GPU form
+// of the same idea is src/grid_Cuda_Optim.cu:1085-2160, plain SIMT with a __shared__ tile
+// and per-plane __syncthreads).
+//
+// Design (one CTA = one TX x TY tile of (i1, i2) marching over a chunk of i3 planes):
+//  * a producer warp streams the planes of the input grid into a ring of shared-memory
+//    tiles with TMA (cp.async.bulk.tensor.3d, no cluster multicast): plane tile with the
+//    x/y halos the operator needs, plus, for the pressure update, the prn and coef tiles
+//    of the output plane. Full/empty mbarriers hand the slots between producer and
+//    consumers; the ring runs PF planes ahead of the consumers;
+//  * consumer threads own VX consecutive i1 points (16 bytes, one vector shared-memory
+//    load) of VY consecutive rows and keep the 2R+1 values of each point along i3 in a
+//    register queue, so every plane is read from HBM once (plus the chunk's z-halo);
+//  * the x/y derivatives read the staged tile of the centre plane, which the ring keeps
+//    resident for R iterations after it arrives;
+//  * every operation is a separately rounded IEEE operation in the reference's order,
+//    so the results are bit-identical to the reference CPU path.
+// MODE_STEP fuses applyBoundaryCondition(prc, ANTI_MIRROR) into the pressure update: every
+// value the stencils read is the value after the boundary condition, built from the raw
+// tile (halos from mirror points in the same tile, boundary lines and planes as zero, z-halo
+// planes loaded from their mirror planes). The kernel never writes prc, so every CTA reads
+// the raw values; the boundary planes' zeros are written by a separate launch afterwards.
+// Every wait on an mbarrier is bounded by a time limit: a CTA that gives up records an
+// error flag (read by b200_device_status) and returns after its issued copies have landed.
+//
+// This header holds the kernel template and its launcher; b200_zmarch_{pressure,laplacian,
+// d2}.cu instantiate them per operator and b200_stencil_zmarch.cu dispatches and tunes.
+#pragma once
+
+#include <cuda.h>
+
+#include <cstring>
+
+#include "b200_stencil.cuh"
+
+namespace b200 {
+
+namespace {
+
+// ---- PTX wrappers -------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+	return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+			: "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+			"r"(bytes)
+			: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+	uint32_t ok;
+	asm volatile(
+			"{\n\t.reg .pred p;\n\t"
+			"mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+			"selp.u32 %0, 1, 0, p;\n\t}"
+			: "=r"(ok)
+			: "r"(smem_u32(bar)), "r"(parity)
+			: "memory");
+	return ok != 0;
+}
+
+// CTA-local named barrier over `nthreads` threads (a multiple of 32).
+__device__ __forceinline__ void named_barrier_sync(int id, int nthreads)
+{
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns()
+{
+	uint64_t t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// Wait for the completion of the mbarrier phase of the given parity, at most until
+// `deadline` (global timer, ns). Returns false when the time ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t deadline)
+{
+	if (mbar_try_wait(bar, parity)) return true;
+	for (uint32_t n = 1;; ++n) {
+		if (mbar_try_wait(bar, parity)) return true;
+		if ((n & 63u) == 0 && global_timer_ns() > deadline) return false;
+	}
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, int x, int y, int z,
+		uint64_t* bar)
+{
+	asm volatile(
+			"cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+			" [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+			"l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+			: "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* tm)
+{
+	asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");
+}
+
+// ---- vector shared-memory loads (16 bytes) converted to the compute type --------------------------
+template <typename S, typename C, int N>
+__device__ __forceinline__ void lds_vec(const S* p, C* out)
+{
+	static_assert(N * sizeof(S) % 16 == 0, "vector of 16-byte multiples");
+#pragma unroll
+	for (int b = 0; b < N * (int)sizeof(S) / 16; b++) {
+		const uint4 raw = reinterpret_cast<const uint4*>(p)[b];
+		const S* v = reinterpret_cast<const S*>(&raw);
+#pragma unroll
+		for (int i = 0; i < 16 / (int)sizeof(S); i++)
+			out[b * (16 / sizeof(S)) + i] = Storage<S>::load(v[i]);
+	}
+}
+
+constexpr int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// ---- kernel configuration -----------------------------------------------------------------------
+template <typename S, int R_, int MODE_, int TX_, int TY_, int VY_, int PF_, bool EXACT_ = true,
+		int MINB_ = 0>
+struct ZCfg {
+	using Stor = S;
+	using C = typename Storage<S>::C;
+	static constexpr bool EXACT = EXACT_;
+	static constexpr int R = R_;
+	static constexpr int MODE = MODE_;
+	static constexpr int TX = TX_, TY = TY_, VY = VY_, PF = PF_;
+	static constexpr int VX = 16 / sizeof(S);
+	static constexpr bool BC = (MODE == MODE_STEP);          // anti-mirror BC fused in
+	static constexpr bool XH = (MODE == MODE_D2_AXIS1 || MODE >= MODE_LAPLACIAN);
+	static constexpr bool YH = (MODE == MODE_D2_AXIS2 || MODE >= MODE_LAPLACIAN);
+	static constexpr bool ZQ = (MODE == MODE_D2_AXIS3 || MODE >= MODE_LAPLACIAN);
+	static constexpr bool P = (MODE == MODE_PRESSURE || MODE == MODE_STEP);
+	static constexpr int R4 = XH ? round_up(R, VX) : 0;     // x halo, whole vectors
+	static constexpr int RY = YH ? R : 0;
+	static constexpr int RZ = ZQ ? R : 0;
+	static constexpr int BX = TX + 2 * R4;
+	static constexpr int BY = TY + 2 * RY;
+	static constexpr int NSU = RZ + 1 + PF;                  // input-tile ring
+	static constexpr int NSP = P ? 1 + PF : 1;               // prn/coef ring
+	static constexpr int U_BYTES = BX * BY * (int)sizeof(S);
+	static constexpr int U_STRIDE = round_up(U_BYTES, 128);
+	static constexpr int PT_BYTES = TX * TY * (int)sizeof(S);
+	static constexpr int PT_STRIDE = round_up(PT_BYTES, 128);
+	static constexpr int NTX = TX / VX;
+	static constexpr int NC = NTX * (TY / VY);              // consumer threads
+	static constexpr int NWC = NC / 32;                      // consumer warps
+	static constexpr int NT = NC + 32;                       // + one producer warp
+	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * 2 * PT_STRIDE : 0) +
+	                            (2 * NSU + 2 * NSP) * 8;
+	// CTAs per SM the launch bounds ask for (registers follow: an SM has four sub-partitions
+	// of 16K registers and spreads a CTA's warps over them). Two CTAs per SM for R <= 4 with
+	// 8-warp CTAs; wider stencils keep their longer z queue in registers at one CTA per SM.
+	static constexpr int MINB = MINB_ > 0 ? MINB_ : ((NT <= 256 && R <= 4) ? 2 : 1);
+	static_assert(TX % VX == 0 && TY % VY == 0 && NC % 32 == 0, "tile shape");
+	static_assert(BX <= 256 && BY <= 256, "TMA box limit");
+	static_assert((BX * sizeof(S)) % 16 == 0 && (TX * sizeof(S)) % 16 == 0, "TMA inner extent");
+};
+
+template <typename C>
+struct ZArgs {
+	void* out;                 // w, or prn for the pressure update
+	int64_t n1, n12;
+	int x_start;               // first tile's i1 (16-byte aligned index)
+	int s1, e1, s2, e2, s3, e3;
+	int nz_chunk;
+	C inv2_1, inv2_2, inv2_3;
+	float coef_scale;
+	uint64_t timeout_ns;
+	unsigned int* err;         // device error word (b200_device_status)
+};
+
+
+// Position in a ring of N slots: the slot index and the parity of the slot's use count
+// (the mbarrier phase parity), advanced without integer division.
+template <int N>
+struct Ring {
+	int slot = 0;
+	uint32_t phase = 0;
+	__device__ __forceinline__ void advance()
+	{
+		if (++slot == N) {
+			slot = 0;
+			phase ^= 1u;
+		}
+	}
+};
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
+		const __grid_constant__ CUtensorMap tm_u,
+		const __grid_constant__ CUtensorMap tm_prn, const __grid_constant__ CUtensorMap tm_coef,
+		const ZArgs<typename Cfg::C> a)
+{
+	using S = typename Cfg::Stor;
+	using C = typename Cfg::C;
+	constexpr bool EX = Cfg::EXACT;
+	using A = Arith<EX>;
+	constexpr int R = Cfg::R, VX = Cfg::VX, VY = Cfg::VY, TX = Cfg::TX;
+	constexpr int R4 = Cfg::R4, RY = Cfg::RY, RZ = Cfg::RZ, BX = Cfg::BX;
+	constexpr int NSU = Cfg::NSU, NSP = Cfg::NSP, NC = Cfg::NC;
+	constexpr int UE = Cfg::U_STRIDE / (int)sizeof(S);     // elements between input tiles
+	constexpr int PE = Cfg::PT_STRIDE / (int)sizeof(S);    // elements between prn/coef tiles
+	constexpr unsigned FULL = 0xffffffffu;
+
+	extern __shared__ unsigned char smem_raw[];
+	unsigned char* smem = reinterpret_cast<unsigned char*>(
+			(reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+	S* su = reinterpret_cast<S*>(smem);
+	S* sp = reinterpret_cast<S*>(smem + NSU * Cfg::U_STRIDE);
+	uint64_t* bars = reinterpret_cast<uint64_t*>(
+			smem + NSU * Cfg::U_STRIDE + (Cfg::P ? NSP * 2 * Cfg::PT_STRIDE : 0));
+	uint64_t* full_u = bars;
+	uint64_t* empty_u = bars + NSU;
+	uint64_t* full_p = bars + 2 * NSU;
+	uint64_t* empty_p = full_p + NSP;
+
+	const int tile_x0 = a.x_start + (int)blockIdx.x * TX;
+	const int tile_y0 = a.s2 + (int)blockIdx.y * Cfg::TY;
+	const int z0 = a.s3 + (int)blockIdx.z * a.nz_chunk;
+	const int z1 = min(z0 + a.nz_chunk, a.e3 + 1);
+	const int J = (z1 - z0) + 2 * RZ;          // planes this CTA streams in
+
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < NSU; s++) {
+			mbar_init(&full_u[s], 1);
+			mbar_init(&empty_u[s], Cfg::NWC);
+		}
+		for (int s = 0; s < NSP; s++) {
+			mbar_init(&full_p[s], 1);
+			mbar_init(&empty_p[s], Cfg::NWC);
+		}
+		fence_mbar_init();
+	}
+	__syncthreads();
+	const uint64_t deadline = global_timer_ns() + a.timeout_ns;
+
+	if (threadIdx.x >= NC) {
+		// ---- producer: one thread issues every TMA copy ------------------------------------------
+		if (threadIdx.x != NC) return;
+		prefetch_tmap(&tm_u);
+		if constexpr (Cfg::P) {
+			prefetch_tmap(&tm_prn);
+			prefetch_tmap(&tm_coef);
+		}
+		int issued_u = 0, issued_p = 0;
+		bool ok = true;
+		Ring<NSU> wu;
+		Ring<NSP> wp;
+		for (int j = 0; j < J; ++j) {
+			// slot reuse: wait for the consumers' previous release of this slot
+			if (j >= NSU && !mbar_wait(&empty_u[wu.slot], wu.phase ^ 1u, deadline)) {
+				ok = false;
+				break;
+			}
+			int plane = z0 - RZ + j;
+			if constexpr (Cfg::BC) {
+				// z-halo planes are rebuilt from their mirror planes by the consumers
+				if (plane < a.s3) plane = 2 * a.s3 - plane;
+				else if (plane > a.e3) plane = 2 * a.e3 - plane;
+			}
+			mbar_arrive_expect_tx(&full_u[wu.slot], Cfg::U_BYTES);
+			tma_load_3d(su + wu.slot * UE, &tm_u, tile_x0 - R4, tile_y0 - RY, plane, &full_u[wu.slot]);
+			issued_u = j + 1;
+			wu.advance();
+			if constexpr (Cfg::P) {
+				if (j >= 2 * RZ) {
+					const int o = j - 2 * RZ;
+					if (o >= NSP && !mbar_wait(&empty_p[wp.slot], wp.phase ^ 1u, deadline)) {
+						ok = false;
+						break;
+					}
+					mbar_arrive_expect_tx(&full_p[wp.slot], 2 * Cfg::PT_BYTES);
+					tma_load_3d(sp + (2 * wp.slot) * PE, &tm_prn, tile_x0, tile_y0, z0 + o,
+							&full_p[wp.slot]);
+					tma_load_3d(sp + (2 * wp.slot + 1) * PE, &tm_coef, tile_x0, tile_y0, z0 + o,
+							&full_p[wp.slot]);
+					issued_p = o + 1;
+					wp.advance();
+				}
+			}
+		}
+		if (!ok) atomicOr(a.err, 1u);
+		// every issued copy lands before the CTA may retire its shared memory
+		const uint64_t drain = global_timer_ns() + a.timeout_ns;
+		for (int j = max(0, issued_u - NSU); j < issued_u; ++j)
+			mbar_wait(&full_u[j % NSU], (j / NSU) & 1, drain);
+		for (int o = max(0, issued_p - NSP); o < issued_p; ++o)
+			mbar_wait(&full_p[o % NSP], (o / NSP) & 1, drain);
+		return;
+	}
+
+	// ---- consumers ---------------------------------------------------------------------------
+	const int tid = threadIdx.x;
+	const int lane = tid & 31;
+	const int xl = (tid % Cfg::NTX) * VX;
+	const int yl = (tid / Cfg::NTX) * VY;
+	const int X = tile_x0 + xl;
+	const int Y0 = tile_y0 + yl;
+	C q[2 * RZ + 1][VY][VX];           // values along i3 of this thread's points
+	// `alive` turns false when a bounded wait runs out: the warp then skips all work but keeps
+	// the loop's barrier sequence, so no other warp is left waiting at a named barrier.
+	bool alive = true;
+	Ring<NSU> ru;                      // front plane j
+	Ring<NSU> rc;                      // centre plane j - RZ
+	rc.slot = RZ;                      // stage RZ: first centre plane (RZ < NSU, use 0)
+	Ring<NSP> rp;                      // prn/coef of output plane j - 2 RZ
+
+	// ---- fused boundary condition: per-thread constants, the same for every plane ----
+	// A CTA whose tile (with halos) comes within R of an i1 or i2 boundary line rebuilds, in
+	// shared memory, the values the boundary condition leaves: phase 1 writes the halo points
+	// from their mirror points (i1 halos = -(mirror) before any face; i2 halos = -(mirror)
+	// after the i1 faces zeroed their boundary columns), phase 2 zeroes the boundary lines and,
+	// on a boundary plane, every inner point (reference face order I1, I2, I3). Each thread
+	// owns a fixed list of tile offsets for both phases.
+	constexpr int BYc = Cfg::BY;
+	constexpr int NP1 = Cfg::BC ? (2 * R * BYc + 2 * R * BX + NC - 1) / NC : 1;
+	constexpr int NP2 = Cfg::BC ? (2 * BYc + 2 * BX + NC - 1) / NC : 1;
+	constexpr uint32_t NO_PATCH = 0xFFFFFFFFu, NEG_ZERO = 0xFFFFu;
+	bool near = false;
+	uint32_t p1[NP1];                  // phase 1: (dst << 16) | src, src NEG_ZERO writes -0
+	uint32_t p2[NP2];                  // phase 2: offset to zero
+	uint32_t qline = 0;                // bits over the thread's points that lie on a boundary line
+	if constexpr (Cfg::BC) {
+		const int xs = tile_x0 - R4, xe = tile_x0 + TX + R4 - 1;
+		const int ys = tile_y0 - RY, ye = tile_y0 + Cfg::TY + RY - 1;
+		near = (xs <= a.s1 + R && xe >= a.s1 - R) || (xs <= a.e1 + R && xe >= a.e1 - R) ||
+		       (ys <= a.s2 + R && ye >= a.s2 - R) || (ys <= a.e2 + R && ye >= a.e2 - R);
+#pragma unroll
+		for (int v = 0; v < VY; v++)
+#pragma unroll
+			for (int e = 0; e < VX; e++) {
+				const int x = X + e, y = Y0 + v;
+				if (x == a.s1 || x == a.e1 || y == a.s2 || y == a.e2) qline |= 1u << (v * VX + e);
+			}
+		const int nxband = 2 * R * BYc, nyband = 2 * R * BX;
+#pragma unroll
+		for (int m = 0; m < NP1; m++) {
+			p1[m] = NO_PATCH;
+			const int idx = tid + m * NC;
+			if (!near) continue;
+			if (idx < nxband) {
+				const int side = idx / (R * BYc), rem = idx % (R * BYc);
+				const int kk = rem / BYc + 1, r = rem % BYc;
+				const int y = ys + r;
+				const int ch = (side ? a.e1 + kk : a.s1 - kk) - xs;
+				const int cm = (side ? a.e1 - kk : a.s1 + kk) - xs;
+				if (y >= a.s2 && y <= a.e2 && ch >= 0 && ch < BX && cm >= 0 && cm < BX)
+					p1[m] = (uint32_t)(r * BX + ch) << 16 | (uint32_t)(r * BX + cm);
+			} else if (idx < nxband + nyband) {
+				const int i2 = idx - nxband;
+				const int side = i2 / (R * BX), rem = i2 % (R * BX);
+				const int kk = rem / BX + 1, c = rem % BX;
+				const int x = xs + c;
+				const int rh = (side ? a.e2 + kk : a.s2 - kk) - ys;
+				const int rm = (side ? a.e2 - kk : a.s2 + kk) - ys;
+				if (x >= a.s1 && x <= a.e1 && rh >= 0 && rh < BYc && rm >= 0 && rm < BYc)
+					p1[m] = (uint32_t)(rh * BX + c) << 16 |
+					        ((x == a.s1 || x == a.e1) ? NEG_ZERO : (uint32_t)(rm * BX + c));
+			}
+		}
+#pragma unroll
+		for (int m = 0; m < NP2; m++) {
+			p2[m] = NO_PATCH;
+			const int idx = tid + m * NC;
+			if (!near) continue;
+			if (idx < 2 * BYc) {                       // boundary columns s1, e1
+				const int side = idx / BYc, r = idx % BYc;
+				const int y = ys + r, c = (side ? a.e1 : a.s1) - xs;
+				if (y >= a.s2 && y <= a.e2 && c >= 0 && c < BX) p2[m] = (uint32_t)(r * BX + c);
+			} else if (idx < 2 * BYc + 2 * BX) {       // boundary rows s2, e2
+				const int i2 = idx - 2 * BYc;
+				const int side = i2 / BX, c = i2 % BX;
+				const int x = xs + c, r = (side ? a.e2 : a.s2) - ys;
+				if (x >= a.s1 && x <= a.e1 && r >= 0 && r < BYc) p2[m] = (uint32_t)(r * BX + c);
+			}
+		}
+	}
+
+	for (int j = 0; j < J; ++j) {
+		const int s = ru.slot;
+		if (alive && !__all_sync(FULL, mbar_wait(&full_u[s], ru.phase, deadline))) alive = false;
+		if constexpr (Cfg::ZQ) {
+			if (alive) {
+#pragma unroll
+				for (int i = 0; i < 2 * RZ; i++)
+#pragma unroll
+					for (int v = 0; v < VY; v++)
+#pragma unroll
+						for (int e = 0; e < VX; e++) q[i][v][e] = q[i + 1][v][e];
+				const S* t = su + s * UE;
+#pragma unroll
+				for (int v = 0; v < VY; v++)
+					lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl, q[2 * RZ][v]);
+				if constexpr (Cfg::BC) {
+					// values after the boundary condition: boundary lines and planes are zero; a
+					// z-halo plane (loaded from its mirror) is minus the mirror after the i1/i2
+					// faces zeroed their lines
+					const int plane = z0 - RZ + j;
+					const bool mir = plane < a.s3 || plane > a.e3;
+					const bool zb = plane == a.s3 || plane == a.e3;
+					if (near || mir || zb) {
+#pragma unroll
+						for (int v = 0; v < VY; v++)
+#pragma unroll
+							for (int e = 0; e < VX; e++) {
+								const bool line = (qline >> (v * VX + e)) & 1u;
+								C& val = q[2 * RZ][v][e];
+								if (mir) val = line ? -C(0) : -val;
+								else if (line || zb) val = C(0);
+							}
+					}
+				}
+			}
+		}
+		if (j >= 2 * RZ) {
+			const int o = j - 2 * RZ;
+			const int k = z0 + o;                     // output plane
+			const int sc = Cfg::ZQ ? rc.slot : s;      // slot holding plane k with its halos
+			const S* t = su + sc * UE;
+			const S* pt = nullptr;
+			if constexpr (Cfg::P) {
+				if (alive && !__all_sync(FULL, mbar_wait(&full_p[rp.slot], rp.phase, deadline)))
+					alive = false;
+				pt = sp + (2 * rp.slot) * PE;
+			}
+			const bool kb = Cfg::BC && (k == a.s3 || k == a.e3);
+			if constexpr (Cfg::BC) {
+				if (near || kb) {
+					S* tw = su + sc * UE;
+					if (alive && near) {
+#pragma unroll
+						for (int m = 0; m < NP1; m++) {
+							const uint32_t pe = p1[m];
+							if (pe == NO_PATCH) continue;
+							const uint32_t src = pe & 0xFFFFu;
+							const C mv = src == NEG_ZERO ? C(0) : Storage<S>::load(tw[src]);
+							tw[pe >> 16] = Storage<S>::store(-mv);
+						}
+					}
+					named_barrier_sync(1, NC);   // every consumer warp, alive or not
+					if (alive) {
+						if (near) {
+#pragma unroll
+							for (int m = 0; m < NP2; m++)
+								if (p2[m] != NO_PATCH) tw[p2[m]] = S(0.0f);
+						}
+						if (kb) {                // boundary plane: every inner point is zero
+							const int xs = tile_x0 - R4, ys = tile_y0 - RY;
+							for (int idx = tid; idx < BX * BYc; idx += NC) {
+								const int r = idx / BX, c = idx - r * BX;
+								const int x = xs + c, y = ys + r;
+								if (x >= a.s1 && x <= a.e1 && y >= a.s2 && y <= a.e2) tw[idx] = S(0.0f);
+							}
+						}
+					}
+					named_barrier_sync(1, NC);
+				}
+			}
+			if (alive) {
+				// rows of this thread's columns, plane k: (VY + 2 RY) x VX values (near a
+				// boundary the centre rows come from the patched tile too: a thread's vector
+				// can straddle the last inner point, and its halo part needs the patch)
+				C yv[VY + 2 * RY][VX];
+#pragma unroll
+				for (int r = 0; r < VY + 2 * RY; r++) {
+					const int v = r - RY;
+					if (v >= 0 && v < VY && Cfg::ZQ && !(Cfg::BC && (near || kb))) {
+#pragma unroll
+						for (int e = 0; e < VX; e++) yv[r][e] = q[RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
+					} else {
+						lds_vec<S, C, VX>(t + (yl + r) * BX + R4 + xl, yv[r]);
+					}
+				}
+#pragma unroll
+				for (int v = 0; v < VY; v++) {
+					C res[VX];
+					C dx[VX], dy[VX], dz[VX];
+					if constexpr (Cfg::XH) {
+						C xv[VX + 2 * R4];
+#pragma unroll
+						for (int h = 0; h < R4 / VX; h++)
+							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + xl + h * VX, &xv[h * VX]);
+#pragma unroll
+						for (int e = 0; e < VX; e++) xv[R4 + e] = yv[v + RY][e];
+#pragma unroll
+						for (int h = 0; h < R4 / VX; h++)
+							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl + VX + h * VX,
+									&xv[R4 + VX + h * VX]);
+#pragma unroll
+						for (int e = 0; e < VX; e++)
+							dx[e] = d2_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
+					}
+					if constexpr (Cfg::YH) {
+#pragma unroll
+						for (int e = 0; e < VX; e++)
+							dy[e] = d2_axis<C, R, EX>([&](int kk) { return yv[v + RY + kk][e]; }, a.inv2_2);
+					}
+					if constexpr (Cfg::ZQ) {
+#pragma unroll
+						for (int e = 0; e < VX; e++)
+							dz[e] = d2_axis<C, R, EX>([&](int kk) { return q[RZ + kk][v][e]; }, a.inv2_3);
+					}
+					if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
+#pragma unroll
+						for (int e = 0; e < VX; e++) res[e] = dx[e];
+					} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
+#pragma unroll
+						for (int e = 0; e < VX; e++) res[e] = dy[e];
+					} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
+#pragma unroll
+						for (int e = 0; e < VX; e++) res[e] = dz[e];
+					} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
+#pragma unroll
+						for (int e = 0; e < VX; e++) res[e] = A::add(A::add(dx[e], dy[e]), dz[e]);
+					} else {
+						C pn[VX], cf[VX];
+						lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
+						lds_vec<S, C, VX>(pt + PE + (yl + v) * TX + xl, cf);
+#pragma unroll
+						for (int e = 0; e < VX; e++) {
+							C c = cf[e];
+							if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
+							res[e] = leapfrog<C, EX>(yv[v + RY][e], pn[e], c,
+									A::add(A::add(dx[e], dy[e]), dz[e]));
+						}
+					}
+					const int Y = Y0 + v;
+					if (Y <= a.e2) {
+						S* dst = static_cast<S*>(a.out) + X + (int64_t)Y * a.n1 + (int64_t)k * a.n12;
+						if (X >= a.s1 && X + VX - 1 <= a.e1) {
+							uint4 pk;
+							S* ps = reinterpret_cast<S*>(&pk);
+#pragma unroll
+							for (int e = 0; e < VX; e++) ps[e] = Storage<S>::store(res[e]);
+							*reinterpret_cast<uint4*>(dst) = pk;
+						} else {
+#pragma unroll
+							for (int e = 0; e < VX; e++)
+								if (X + e >= a.s1 && X + e <= a.e1) dst[e] = Storage<S>::store(res[e]);
+						}
+					}
+				}
+			}
+			__syncwarp();
+			if (lane == 0) {
+				mbar_arrive(&empty_u[sc]);
+				if constexpr (Cfg::P) mbar_arrive(&empty_p[rp.slot]);
+			}
+			rc.advance();
+			rp.advance();
+		}
+		if constexpr (Cfg::ZQ) {
+			if (j < RZ || j >= J - RZ) {   // planes that are never a centre plane
+				__syncwarp();
+				if (lane == 0) mbar_arrive(&empty_u[s]);
+			}
+		}
+		ru.advance();
+	}
+	if (!alive && lane == 0) atomicOr(a.err, 2u);
+}
+
+}  // namespace
+
+// ---- host side ------------------------------------------------------------------------------------
+// Tensor map of a 3-D grid with box (bx, by, 1) (b200_stencil_zmarch.cu).
+int make_map(CUtensorMap* m, const void* base, int dtype, const b200_layout* lay, int bx, int by);
+
+namespace {
+
+// planes per CTA: enough CTAs for several waves, long enough chunks to amortise the z-halo
+template <class Cfg>
+int pick_nz_chunk(int ntiles, int nz, int requested)
+{
+	if (requested > 0) return requested < nz ? requested : nz;
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zmarch<Cfg>, Cfg::NT, Cfg::SMEM);
+	if (per_sm < 1) per_sm = 1;
+	const int resident = per_sm * num_sms();
+	int chunk = Cfg::R <= 4 ? 64 : 128;
+	while (chunk > 16 && (int64_t)ntiles * ((nz + chunk - 1) / chunk) < 4 * (int64_t)resident) chunk /= 2;
+	return chunk < nz ? chunk : nz;
+}
+
+template <class Cfg>
+int launch_zmarch(const ZLaunch& L)
+{
+	const b200_layout* lay = L.lay;
+	const b200_field& in = *L.in;
+	const b200_field& out = *L.out;
+	const b200_field* coef = L.coef;
+	const double inv2_1 = L.inv2[0], inv2_2 = L.inv2[1], inv2_3 = L.inv2[2];
+	cudaStream_t s = L.s;
+	using C = typename Cfg::C;
+	int rc = cuda_error(cudaFuncSetAttribute(k_zmarch<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                            Cfg::SMEM), "cudaFuncSetAttribute(k_zmarch)");
+	if (rc) return rc;
+	alignas(64) CUtensorMap tm_u, tm_p, tm_c;
+	if ((rc = make_map(&tm_u, in.data, in.dtype, lay, Cfg::BX, Cfg::BY))) return rc;
+	if (Cfg::P) {
+		if ((rc = make_map(&tm_p, out.data, out.dtype, lay, Cfg::TX, Cfg::TY))) return rc;
+		if ((rc = make_map(&tm_c, coef->data, coef->dtype, lay, Cfg::TX, Cfg::TY))) return rc;
+	} else {
+		tm_p = tm_u;
+		tm_c = tm_u;
+	}
+	ZArgs<C> a;
+	a.out = out.data;
+	a.n1 = lay->n1;
+	a.n12 = lay->n1 * lay->n2;
+	a.x_start = (int)(lay->s1 / Cfg::VX) * Cfg::VX;
+	a.s1 = (int)lay->s1; a.e1 = (int)lay->e1;
+	a.s2 = (int)lay->s2; a.e2 = (int)lay->e2;
+	a.s3 = (int)lay->s3; a.e3 = (int)lay->e3;
+	a.inv2_1 = (C)inv2_1;
+	a.inv2_2 = (C)inv2_2;
+	a.inv2_3 = (C)inv2_3;
+	a.coef_scale = coef ? coef->scale : 1.0f;
+	a.timeout_ns = 2000000000ull;
+	a.err = L.err;
+	const int ntx = (a.e1 + 1 - a.x_start + Cfg::TX - 1) / Cfg::TX;
+	const int nty = (a.e2 - a.s2 + 1 + Cfg::TY - 1) / Cfg::TY;
+	const int nz = a.e3 - a.s3 + 1;
+	a.nz_chunk = pick_nz_chunk<Cfg>(ntx * nty, nz, L.nz_chunk);
+	const int nzc = (nz + a.nz_chunk - 1) / a.nz_chunk;
+	k_zmarch<Cfg><<<dim3(ntx, nty, nzc), Cfg::NT, Cfg::SMEM, s>>>(tm_u, tm_p, tm_c, a);
+	return check_launch("k_zmarch");
+}
+
+
+// Tile shapes the kernel is instantiated with, per storage size and half width:
+// (TX, TY, VY, PF); TX = 16 vectors of 16 bytes. The autotuner (b200_autotune_stencil) picks
+// among them; shape 0 is the default. Consumer-thread counts are 224 (7 warps + the producer
+// warp = 8 warps, two CTAs per SM) or 480 (16 warps, one CTA per SM). Two rows per thread
+// (VY = 2) pay off for R <= 2 only: from R = 3 on, the longer z queue makes the registers,
+// not the shared-memory traffic, the limit (measured on B200).
+template <typename S, int R, int SHAPE> struct Shape;
+template <typename S, int R> struct Shape<S, R, 0> {
+	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 2, MINB = 0; };
+template <typename S, int R> struct Shape<S, R, 1> {
+	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = 30, VY = 1, PF = 2, MINB = 0; };
+template <typename S, int R> struct Shape<S, R, 2> {   // 9 warps; two CTAs per SM for R <= 4
+	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = 16, VY = 1, PF = 2, MINB = R <= 4 ? 2 : 1; };
+
+template <typename S, int R, int MODE, int SHAPE, bool EXACT>
+int launch_shape(const ZLaunch& L)
+{
+	using Sh = Shape<S, R, SHAPE>;
+	return launch_zmarch<ZCfg<S, R, MODE, Sh::TX, Sh::TY, Sh::VY, Sh::PF, EXACT, Sh::MINB>>(L);
+}
+
+// Dispatch storage type, half width, shape and arithmetic for one operator. NSHAPES and
+// WITH_FMA bound the instantiations (the single-axis operators use shape 0, exact only).
+template <int MODE, int NSHAPES, bool WITH_FMA>
+int launch_mode(const ZLaunch& L)
+{
+	return dispatch_order(2 * L.R, [&](auto rt) {
+		constexpr int R = decltype(rt)::value;
+		auto go = [&](auto tag) -> int {
+			using S = decltype(tag);
+			const int shape = (L.shape >= 0 && L.shape < NSHAPES) ? L.shape : 0;
+			const bool exact = L.exact || !WITH_FMA;
+			if (exact) {
+				if (shape == 0) return launch_shape<S, R, MODE, 0, true>(L);
+				if constexpr (NSHAPES > 1) if (shape == 1) return launch_shape<S, R, MODE, 1, true>(L);
+				if constexpr (NSHAPES > 2) return launch_shape<S, R, MODE, 2, true>(L);
+			} else if constexpr (WITH_FMA) {
+				if (shape == 0) return launch_shape<S, R, MODE, 0, false>(L);
+				if constexpr (NSHAPES > 1) if (shape == 1) return launch_shape<S, R, MODE, 1, false>(L);
+				if constexpr (NSHAPES > 2) return launch_shape<S, R, MODE, 2, false>(L);
+			}
+			return set_error(B200_ERR_ARG, "stencil shape %d", shape);
+		};
+		if (L.in->dtype == B200_F64) return go(double{});
+		return go(float{});
+	});
+}
+
+}  // namespace
+}  // namespace b200

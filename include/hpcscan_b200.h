@@ -133,7 +133,14 @@ int b200_apply_boundary(const b200_layout* lay, b200_field u, int bc_type, int f
 		void* stream);
 
 /* Propagator_Ac2::computeWavefieldNextTimeStep for one rank (src/propagator_Ac2.cpp:366-395):
- * applyBoundaryCondition(prc) then computePressureWithFD(prn, prc), in one call. */
+ * applyBoundaryCondition(prc) then computePressureWithFD(prn, prc), in one call. For 3-D
+ * FP32/FP64 grids with at least halo + 2 inner points per axis, once selected by
+ * b200_autotune_stencil or b200_set_stencil_config (op 6), the boundary condition is fused into
+ * the pressure kernel (the anti-mirror values are built inside its shared-memory tiles),
+ * followed by a small kernel that writes the boundary planes' zeros into prc; prn and the inner
+ * points of prc end up bit-identical to the two separate calls, and prc's halo points are left
+ * as they were (the next boundary condition rebuilds them before any read). Otherwise it runs
+ * the boundary-condition kernels and the pressure kernel back to back. */
 int b200_propagate_step(const b200_layout* lay, int order, b200_field prn, b200_field prc,
 		b200_field coef, double inv2_1, double inv2_2, double inv2_3, int bc_type, void* stream);
 
@@ -162,6 +169,44 @@ int b200_min_max(const b200_layout* lay, b200_field u, const b200_box* box, doub
 int b200_l1_sums_separable(const b200_layout* lay, b200_field u, const b200_box* box,
 		const double* v1, const double* v2, const double* v3, double amp, int ref_dtype,
 		double* sum_abs_diff, double* sum_abs_ref, void* stream);
+
+/* ---- arithmetic mode and tuning ---------------------------------------------------------------
+ * B200_ARITH_EXACT (default): every multiply and add of the stencil operators is a separately
+ * rounded IEEE operation in the reference's evaluation order, so FP32/FP64 results are
+ * bit-identical to the reference CPU path built without FP contraction.
+ * B200_ARITH_FMA: the same expression order with fused multiply-adds (fewer instructions;
+ * results differ from the reference in the last bits). Applies to the 3-D z-marching
+ * pressure and Laplacian kernels. No reference counterpart. */
+#define B200_ARITH_EXACT 0
+#define B200_ARITH_FMA   1
+int b200_set_arith_mode(int mode);
+int b200_get_arith_mode(int* mode);
+
+/* Operators for the tuning calls: 1..3 = FD_D2_N1..N3, 4 = FD_LAPLACIAN,
+ * 5 = computePressureWithFD, 6 = the fused propagator step. */
+#define B200_OP_FD_D2_N1     1
+#define B200_OP_FD_D2_N2     2
+#define B200_OP_FD_D2_N3     3
+#define B200_OP_LAPLACIAN    4
+#define B200_OP_PRESSURE     5
+#define B200_OP_STEP         6    /* b200_propagate_step with the anti-mirror BC */
+
+/* Tile shape (0..2 for the Laplacian, pressure and step kernels, 0 otherwise) and planes per
+ * CTA (0 = heuristic) used by the 3-D kernels for (dtype, order, op); shape -1 restores the
+ * untuned defaults. For op 6 a shape selects the fused step kernel (untuned, b200_propagate_step
+ * runs the boundary-condition kernels and the pressure kernel). Replaces the reference's manual
+ * cache-block flags -cb1/-cb2/-cb3 (src/config.cpp; src/grid_Cuda_Optim.cu:2163-2211). */
+int b200_set_stencil_config(int dtype, int order, int op, int shape, int nz_chunk);
+int b200_get_stencil_config(int dtype, int order, int op, int* shape, int* nz_chunk);
+
+/* Autotuner: times every tile shape and plane-chunk candidate of the 3-D kernel for `op` on
+ * scratch grids of this layout (allocated and freed here), records the fastest for later
+ * launches of (dtype, order, op) and returns it. For op 6 it also times the boundary-condition
+ * kernels + the tuned pressure kernel and keeps the fused kernel only if it is faster
+ * (*best_shape = -1 then). Synchronous. No reference counterpart (the reference sweeps -cb
+ * flags by script: script/testCase_FD_D2/cacheBlkAnalysis). */
+int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, int reps,
+		int* best_shape, int* best_chunk, double* best_ms);
 
 /* ---- diagnostics ----------------------------------------------------------------------------
  * Device-side error word of the library's kernels (0 = none; bit 0: a producer gave up a

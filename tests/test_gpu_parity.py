@@ -265,3 +265,64 @@ def test_fused_check_equals_materialised_reference(gpu):
         assert ia == ib
         np.testing.assert_allclose([s1a, s2a], [s1b, s2b], rtol=1e-12)
     assert a.err_test_case == b.err_test_case
+
+
+# ---- the fused propagator step (boundary condition inside the pressure kernel) -----------------
+
+STEP_LAYOUTS = [L.b200_layout(3, 37, 20, 23, order=8), L.b200_layout(3, 70, 33, 41, order=16),
+                L.b200_layout(3, 130, 37, 150, order=8), L.b200_layout(3, 66, 49, 35, order=4),
+                L.b200_layout(3, 21, 22, 20, order=2), L.b200_layout(3, 45, 27, 29, order=6),
+                L.b200_layout(3, 52, 31, 40, order=12, prec="f64"),
+                L.b200_layout(3, 37, 20, 23, order=8, prec="f64"),
+                L.b200_layout(3, 33, 40, 22, order=14), L.b200_layout(3, 29, 21, 25, order=10)]
+
+
+def propagate_step(lay, prn, prc, coef, samp):
+    import ctypes
+    from hpcscan_b200 import _lib
+    cl = _lib.Layout(*lay.c_struct_fields())
+    i1, i2, i3 = L.inv2_spacing(samp, lay.prec)
+    _lib.call("b200_propagate_step", ctypes.byref(cl), lay.order, prn.c_field(), prc.c_field(),
+              coef.c_field(), i1, i2, i3, 1, None)
+
+
+@pytest.mark.parametrize("lay", STEP_LAYOUTS, ids=lay_id)
+@pytest.mark.parametrize("shape,chunk", [(0, 0), (1, 16), (2, 7)])
+def test_fused_step_bitexact(gpu, oracle, lay, shape, chunk):
+    """b200_propagate_step (BC fused into the pressure kernel) == applyBoundaryCondition +
+    computePressureWithFD of the oracle, bit for bit, over several steps; prc's inner points
+    (with the zeroed boundary planes) too. Every tile shape, with z-chunks that put chunk
+    edges next to the boundary planes."""
+    from hpcscan_b200 import _lib
+    _lib.call("b200_set_stencil_config", _lib.DTYPE_CODE[lay.prec], lay.order, _lib.OP_STEP,
+              shape, chunk)
+    try:
+        prc, prn, coef = rand_field(lay, 12), rand_field(lay, 13), np.abs(rand_field(lay, 14)) * 1e-3
+        samp = L.Sampling((0.02, 0.03, 0.025), (0.0, 0.0, 0.0))
+        inv2 = L.inv2_spacing(samp, lay.prec)
+        Prc, Prn, Coef = dev(lay, prc, samp), dev(lay, prn, samp), dev(lay, coef, samp)
+        a, b = prn.copy(), prc.copy()
+        for it in range(3):
+            propagate_step(lay, Prn, Prc, Coef, samp)
+            oracle.apply_bc(lay, b)
+            oracle.compute_pressure(lay, a, b, coef, inv2)
+            assert np.array_equal(bits(lay.inner(Prn.to_numpy())), bits(lay.inner(a))), it
+            assert np.array_equal(bits(lay.inner(Prc.to_numpy())), bits(lay.inner(b))), it
+            Prn, Prc = Prc, Prn
+            a, b = b, a
+        assert device_status() == 0
+    finally:
+        _lib.call("b200_set_stencil_config", _lib.DTYPE_CODE[lay.prec], lay.order, _lib.OP_STEP, -1, 0)
+
+
+def test_fused_step_small_grid_falls_back(gpu, oracle):
+    """Fewer than halo + 2 inner points on an axis: the two operators run back to back."""
+    lay = L.b200_layout(3, 30, 9, 25, order=16)
+    prc, prn, coef = rand_field(lay, 15), rand_field(lay, 16), np.abs(rand_field(lay, 17)) * 1e-3
+    samp = L.Sampling((0.02, 0.03, 0.025), (0.0, 0.0, 0.0))
+    Prc, Prn, Coef = dev(lay, prc, samp), dev(lay, prn, samp), dev(lay, coef, samp)
+    propagate_step(lay, Prn, Prc, Coef, samp)
+    oracle.apply_bc(lay, prc)
+    oracle.compute_pressure(lay, prn, prc, coef, L.inv2_spacing(samp, lay.prec))
+    assert np.array_equal(bits(Prn.to_numpy()), bits(prn))
+    assert np.array_equal(bits(Prc.to_numpy()), bits(prc))
