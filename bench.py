@@ -88,59 +88,69 @@ def profiled_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled in-process through NVML every 20 ms; start it
+    before the warm-up so that no NVML start-up falls into the timed region, and mark the
+    timed region with begin()/end()."""
+    PERIOD_S = 0.02
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+        self.samples = []          # (t, sm_mhz, max_mhz, reasons bitmask)
+        self.window = None
+        self.ok = False
+        self.stop_ev = threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
-                stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+            self.t = threading.Thread(target=self._run, daemon=True)
             self.t.start()
+            time.sleep(0.2)
         except Exception:
-            self.proc = None
+            self.ok = False
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self.stop_ev.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((time.perf_counter(), sm, rs))
+            except Exception:
+                pass
+            time.sleep(self.PERIOD_S)
+
+    def begin(self):
+        self.t0 = time.perf_counter()
+
+    def end(self):
+        self.window = (self.t0, time.perf_counter())
+        time.sleep(self.PERIOD_S * 2)
 
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self.stop_ev.set()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+        if not self.ok:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        nv = self.nv
+        t0, t1 = self.window
+        sel = [x for x in self.samples if t0 - self.PERIOD_S <= x[0] <= t1 + self.PERIOD_S]
+        if not sel:
+            sel = self.samples[-3:]
+        names = {"hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+                 "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+                 "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+                 "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4)}
+        reasons = sorted({n for _, _, rs in sel for n, bit in names.items() if rs & bit})
+        return {"sm_mhz": statistics.median([x[1] for x in sel]), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(sel)}
 
 
 # ---- reference CPU path -------------------------------------------------------------------------
@@ -250,19 +260,21 @@ def b200_arm(a):
             kev[i][1].record(stream)
         prn, prc = prc, prn
 
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clk:
+        for _ in range(a.warmup):
+            step()
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk.begin()
         e0.record(stream)
         for i in range(a.steps):
             step(i)
         e1.record(stream)
         torch.cuda.synchronize()
+        clk.end()
     ms = e0.elapsed_time(e1)
     kern_ms = [s.elapsed_time(e) for s, e in kev]
     st = ctypes.c_int()

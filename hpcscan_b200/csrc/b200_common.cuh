@@ -73,11 +73,85 @@ template <> struct Arith<true> {
 	static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 	static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 	static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+	// acc + c * s, two roundings
+	template <typename C> static __device__ __forceinline__ C mac(C acc, C c, C s)
+	{
+		return add(acc, mul(c, s));
+	}
 };
+// EXACT = false: multiply-adds are fused (one rounding). The library is compiled with
+// -fmad=false, so the fusions are exactly the explicit fma calls here.
 template <> struct Arith<false> {
 	template <typename C> static __device__ __forceinline__ C mul(C a, C b) { return a * b; }
 	template <typename C> static __device__ __forceinline__ C add(C a, C b) { return a + b; }
 	template <typename C> static __device__ __forceinline__ C sub(C a, C b) { return a - b; }
+	template <typename C> static __device__ __forceinline__ C mac(C acc, C c, C s)
+	{
+		return fma(c, s, acc);
+	}
+};
+
+// ---- packed FP32 pairs (sm_100 two-wide add/sub/mul/fma) --------------------------------------
+// PTX add/sub/mul/fma.rn.f32x2 round each component like the scalar .rn instruction. The
+// assembler does, however, fuse a two-wide multiply into a following two-wide add (measured on
+// sm_100a with explicit .rn and with --fmad=false), so the separately rounded arithmetic keeps
+// its products scalar (__fmul_rn) and packs only the additions: bit-identical to the scalar path.
+__device__ __forceinline__ float2 f2_op_add(float2 a, float2 b)
+{
+	float2 d;
+	asm("{\n\t.reg .b64 x, y, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+	    "add.rn.f32x2 z, x, y;\n\tmov.b64 {%0, %1}, z;\n\t}"
+	    : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+	return d;
+}
+__device__ __forceinline__ float2 f2_op_sub(float2 a, float2 b)
+{
+	float2 d;
+	asm("{\n\t.reg .b64 x, y, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+	    "sub.rn.f32x2 z, x, y;\n\tmov.b64 {%0, %1}, z;\n\t}"
+	    : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+	return d;
+}
+__device__ __forceinline__ float2 f2_op_mul(float2 a, float2 b)
+{
+	float2 d;
+	asm("{\n\t.reg .b64 x, y, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+	    "mul.rn.f32x2 z, x, y;\n\tmov.b64 {%0, %1}, z;\n\t}"
+	    : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+	return d;
+}
+// a * b + c with one rounding per component
+__device__ __forceinline__ float2 f2_op_fma(float2 a, float2 b, float2 c)
+{
+	float2 d;
+	asm("{\n\t.reg .b64 x, y, w, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+	    "mov.b64 w, {%6, %7};\n\tfma.rn.f32x2 z, x, y, w;\n\tmov.b64 {%0, %1}, z;\n\t}"
+	    : "=f"(d.x), "=f"(d.y)
+	    : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+	return d;
+}
+
+template <bool EXACT> struct Arith2;
+template <> struct Arith2<true> {
+	static __device__ __forceinline__ float2 mul(float2 a, float2 b)
+	{
+		return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+	}
+	static __device__ __forceinline__ float2 add(float2 a, float2 b) { return f2_op_add(a, b); }
+	static __device__ __forceinline__ float2 sub(float2 a, float2 b) { return f2_op_sub(a, b); }
+	static __device__ __forceinline__ float2 mac(float2 acc, float2 c, float2 s)
+	{
+		return f2_op_add(acc, mul(c, s));
+	}
+};
+template <> struct Arith2<false> {
+	static __device__ __forceinline__ float2 mul(float2 a, float2 b) { return f2_op_mul(a, b); }
+	static __device__ __forceinline__ float2 add(float2 a, float2 b) { return f2_op_add(a, b); }
+	static __device__ __forceinline__ float2 sub(float2 a, float2 b) { return f2_op_sub(a, b); }
+	static __device__ __forceinline__ float2 mac(float2 acc, float2 c, float2 s)
+	{
+		return f2_op_fma(c, s, acc);
+	}
 };
 
 // ---- FD_D2 coefficients (reference src/fdm.h:277-545), exact rationals --------------------------
@@ -120,16 +194,45 @@ __device__ __forceinline__ C d2_axis(F v, C inv2)
 	if constexpr (R == 1) {
 		return A::mul(A::add(A::add(acc, v(1)), v(-1)), inv2);
 	} else {
-		acc = A::add(acc, A::mul(d2c<C, R, 1>(), A::add(v(1), v(-1))));
-		acc = A::add(acc, A::mul(d2c<C, R, 2>(), A::add(v(2), v(-2))));
-		if constexpr (R >= 3) acc = A::add(acc, A::mul(d2c<C, R, 3>(), A::add(v(3), v(-3))));
-		if constexpr (R >= 4) acc = A::add(acc, A::mul(d2c<C, R, 4>(), A::add(v(4), v(-4))));
-		if constexpr (R >= 5) acc = A::add(acc, A::mul(d2c<C, R, 5>(), A::add(v(5), v(-5))));
-		if constexpr (R >= 6) acc = A::add(acc, A::mul(d2c<C, R, 6>(), A::add(v(6), v(-6))));
-		if constexpr (R >= 7) acc = A::add(acc, A::mul(d2c<C, R, 7>(), A::add(v(7), v(-7))));
-		if constexpr (R >= 8) acc = A::add(acc, A::mul(d2c<C, R, 8>(), A::add(v(8), v(-8))));
+		acc = A::mac(acc, d2c<C, R, 1>(), A::add(v(1), v(-1)));
+		acc = A::mac(acc, d2c<C, R, 2>(), A::add(v(2), v(-2)));
+		if constexpr (R >= 3) acc = A::mac(acc, d2c<C, R, 3>(), A::add(v(3), v(-3)));
+		if constexpr (R >= 4) acc = A::mac(acc, d2c<C, R, 4>(), A::add(v(4), v(-4)));
+		if constexpr (R >= 5) acc = A::mac(acc, d2c<C, R, 5>(), A::add(v(5), v(-5)));
+		if constexpr (R >= 6) acc = A::mac(acc, d2c<C, R, 6>(), A::add(v(6), v(-6)));
+		if constexpr (R >= 7) acc = A::mac(acc, d2c<C, R, 7>(), A::add(v(7), v(-7)));
+		if constexpr (R >= 8) acc = A::mac(acc, d2c<C, R, 8>(), A::add(v(8), v(-8)));
 		return A::mul(acc, inv2);
 	}
+}
+
+// d2_axis for a pair of points (packed FP32), same association and rounding per component.
+template <int R, bool EXACT, typename F>
+__device__ __forceinline__ float2 d2_axis2(F v, float2 inv2)
+{
+	using A = Arith2<EXACT>;
+	auto cf = [](float c) { return make_float2(c, c); };
+	float2 acc = A::mul(cf(d2c<float, R, 0>()), v(0));
+	if constexpr (R == 1) {
+		return A::mul(A::add(A::add(acc, v(1)), v(-1)), inv2);
+	} else {
+		acc = A::mac(acc, cf(d2c<float, R, 1>()), A::add(v(1), v(-1)));
+		acc = A::mac(acc, cf(d2c<float, R, 2>()), A::add(v(2), v(-2)));
+		if constexpr (R >= 3) acc = A::mac(acc, cf(d2c<float, R, 3>()), A::add(v(3), v(-3)));
+		if constexpr (R >= 4) acc = A::mac(acc, cf(d2c<float, R, 4>()), A::add(v(4), v(-4)));
+		if constexpr (R >= 5) acc = A::mac(acc, cf(d2c<float, R, 5>()), A::add(v(5), v(-5)));
+		if constexpr (R >= 6) acc = A::mac(acc, cf(d2c<float, R, 6>()), A::add(v(6), v(-6)));
+		if constexpr (R >= 7) acc = A::mac(acc, cf(d2c<float, R, 7>()), A::add(v(7), v(-7)));
+		if constexpr (R >= 8) acc = A::mac(acc, cf(d2c<float, R, 8>()), A::add(v(8), v(-8)));
+		return A::mul(acc, inv2);
+	}
+}
+
+template <bool EXACT>
+__device__ __forceinline__ float2 leapfrog2(float2 prc, float2 prn, float2 coef, float2 lap)
+{
+	using A = Arith2<EXACT>;
+	return A::mac(A::sub(A::mul(make_float2(2.0f, 2.0f), prc), prn), coef, lap);
 }
 
 // Leapfrog update of computePressureWithFD: (2 prc - prn) + coef * lap.
@@ -137,7 +240,7 @@ template <typename C, bool EXACT>
 __device__ __forceinline__ C leapfrog(C prc, C prn, C coef, C lap)
 {
 	using A = Arith<EXACT>;
-	return A::add(A::sub(A::mul(static_cast<C>(2.0), prc), prn), A::mul(coef, lap));
+	return A::mac(A::sub(A::mul(static_cast<C>(2.0), prc), prn), coef, lap);
 }
 
 // Dispatch a runtime FD order to a compile-time half width R.

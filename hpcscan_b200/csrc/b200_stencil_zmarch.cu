@@ -69,17 +69,19 @@ std::mutex g_tune_mutex;
 int g_arith = B200_ARITH_EXACT;
 
 // Untuned defaults: the fastest shape measured at 512^3 on B200 for each storage type and
-// half width (FP32: two-row 28x64 tiles up to R = 2, 9-warp 16x64 tiles for R = 3..4,
-// 30x64 tiles with 128-plane chunks beyond; FP64: 14x32 tiles up to R = 4).
+// half width (FP32: two-row 28x64 tiles up to R = 2, 14x64 tiles with 128-plane chunks for
+// R = 3..4, 9-warp 16x64 tiles beyond, where the 30-row tiles run out of registers; FP64:
+// 14x32 tiles, 30x32 tiles for R = 5..7; at R = 8 those exceed the shared memory).
 Tuned default_tuning(int dtype, int R)
 {
 	Tuned t;
 	if (dtype == B200_F64) {
-		t.shape = R <= 4 ? 0 : 1;
+		t.shape = (R <= 4 || R == 8) ? 0 : 1;
+		t.nz_chunk = R > 4 ? 128 : 0;
 	} else {
-		t.shape = R <= 2 ? 0 : (R <= 4 ? 2 : 1);
+		t.shape = R <= 4 ? 0 : 2;
+		t.nz_chunk = (R >= 3 && R <= 4) ? 128 : 0;
 	}
-	t.nz_chunk = R > 4 ? 128 : 0;
 	return t;
 }
 
@@ -264,7 +266,10 @@ int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, 
 			if (c > nz) continue;
 			L.shape = sh;
 			L.nz_chunk = c;
-			if ((rc = launch(L))) break;      // warm-up (and first-use module load)
+			if ((rc = launch(L))) {           // warm-up (and first-use module load)
+				if (rc == B200_ERR_UNSUPPORTED) rc = B200_OK;   // shape does not fit: skip it
+				break;
+			}
 			if ((rc = cuda_error(cudaEventRecord(e0, s), "cudaEventRecord"))) break;
 			for (int r = 0; r < reps && !rc; r++) rc = launch(L);
 			if (rc) break;

@@ -496,9 +496,9 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 #pragma unroll
 				for (int v = 0; v < VY; v++) {
 					C res[VX];
-					C dx[VX], dy[VX], dz[VX];
+					// x-stencil vector of row v: left halo vectors, centre, right halo vectors
+					C xv[Cfg::XH ? VX + 2 * R4 : 1];
 					if constexpr (Cfg::XH) {
-						C xv[VX + 2 * R4];
 #pragma unroll
 						for (int h = 0; h < R4 / VX; h++)
 							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + xl + h * VX, &xv[h * VX]);
@@ -508,42 +508,91 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 						for (int h = 0; h < R4 / VX; h++)
 							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl + VX + h * VX,
 									&xv[R4 + VX + h * VX]);
-#pragma unroll
-						for (int e = 0; e < VX; e++)
-							dx[e] = d2_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
 					}
-					if constexpr (Cfg::YH) {
+					if constexpr (std::is_same_v<C, float> && VX % 2 == 0) {
+						// FP32: pairs of points with the two-wide instructions
+						using A2 = Arith2<EX>;
+						const float2 i1 = make_float2(a.inv2_1, a.inv2_1);
+						const float2 i2 = make_float2(a.inv2_2, a.inv2_2);
+						const float2 i3 = make_float2(a.inv2_3, a.inv2_3);
 #pragma unroll
-						for (int e = 0; e < VX; e++)
-							dy[e] = d2_axis<C, R, EX>([&](int kk) { return yv[v + RY + kk][e]; }, a.inv2_2);
-					}
-					if constexpr (Cfg::ZQ) {
-#pragma unroll
-						for (int e = 0; e < VX; e++)
-							dz[e] = d2_axis<C, R, EX>([&](int kk) { return q[RZ + kk][v][e]; }, a.inv2_3);
-					}
-					if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
-#pragma unroll
-						for (int e = 0; e < VX; e++) res[e] = dx[e];
-					} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
-#pragma unroll
-						for (int e = 0; e < VX; e++) res[e] = dy[e];
-					} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
-#pragma unroll
-						for (int e = 0; e < VX; e++) res[e] = dz[e];
-					} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
-#pragma unroll
-						for (int e = 0; e < VX; e++) res[e] = A::add(A::add(dx[e], dy[e]), dz[e]);
+						for (int pp = 0; pp < VX / 2; pp++) {
+							const int e = 2 * pp;
+							float2 dx = make_float2(0.f, 0.f), dy = dx, dz = dx, r2;
+							if constexpr (Cfg::XH)
+								dx = d2_axis2<R, EX>([&](int kk) {
+									return make_float2(xv[R4 + e + kk], xv[R4 + e + 1 + kk]); }, i1);
+							if constexpr (Cfg::YH)
+								dy = d2_axis2<R, EX>([&](int kk) {
+									return make_float2(yv[v + RY + kk][e], yv[v + RY + kk][e + 1]); }, i2);
+							if constexpr (Cfg::ZQ)
+								dz = d2_axis2<R, EX>([&](int kk) {
+									return make_float2(q[RZ + kk][v][e], q[RZ + kk][v][e + 1]); }, i3);
+							if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
+								r2 = dx;
+							} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
+								r2 = dy;
+							} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
+								r2 = dz;
+							} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
+								r2 = A2::add(A2::add(dx, dy), dz);
+							} else {
+								float pn[2], cf[2];
+								pn[0] = Storage<S>::load(pt[(yl + v) * TX + xl + e]);
+								pn[1] = Storage<S>::load(pt[(yl + v) * TX + xl + e + 1]);
+								cf[0] = Storage<S>::load(pt[PE + (yl + v) * TX + xl + e]);
+								cf[1] = Storage<S>::load(pt[PE + (yl + v) * TX + xl + e + 1]);
+								if (a.coef_scale != 1.0f) {
+									cf[0] = cf[0] * a.coef_scale;
+									cf[1] = cf[1] * a.coef_scale;
+								}
+								r2 = leapfrog2<EX>(make_float2(yv[v + RY][e], yv[v + RY][e + 1]),
+										make_float2(pn[0], pn[1]), make_float2(cf[0], cf[1]),
+										A2::add(A2::add(dx, dy), dz));
+							}
+							res[e] = r2.x;
+							res[e + 1] = r2.y;
+						}
 					} else {
-						C pn[VX], cf[VX];
-						lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
-						lds_vec<S, C, VX>(pt + PE + (yl + v) * TX + xl, cf);
+						C dx[VX], dy[VX], dz[VX];
+						if constexpr (Cfg::XH) {
 #pragma unroll
-						for (int e = 0; e < VX; e++) {
-							C c = cf[e];
-							if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
-							res[e] = leapfrog<C, EX>(yv[v + RY][e], pn[e], c,
-									A::add(A::add(dx[e], dy[e]), dz[e]));
+							for (int e = 0; e < VX; e++)
+								dx[e] = d2_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
+						}
+						if constexpr (Cfg::YH) {
+#pragma unroll
+							for (int e = 0; e < VX; e++)
+								dy[e] = d2_axis<C, R, EX>([&](int kk) { return yv[v + RY + kk][e]; }, a.inv2_2);
+						}
+						if constexpr (Cfg::ZQ) {
+#pragma unroll
+							for (int e = 0; e < VX; e++)
+								dz[e] = d2_axis<C, R, EX>([&](int kk) { return q[RZ + kk][v][e]; }, a.inv2_3);
+						}
+						if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
+#pragma unroll
+							for (int e = 0; e < VX; e++) res[e] = dx[e];
+						} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
+#pragma unroll
+							for (int e = 0; e < VX; e++) res[e] = dy[e];
+						} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
+#pragma unroll
+							for (int e = 0; e < VX; e++) res[e] = dz[e];
+						} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
+#pragma unroll
+							for (int e = 0; e < VX; e++) res[e] = A::add(A::add(dx[e], dy[e]), dz[e]);
+						} else {
+							C pn[VX], cf[VX];
+							lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
+							lds_vec<S, C, VX>(pt + PE + (yl + v) * TX + xl, cf);
+#pragma unroll
+							for (int e = 0; e < VX; e++) {
+								C c = cf[e];
+								if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
+								res[e] = leapfrog<C, EX>(yv[v + RY][e], pn[e], c,
+										A::add(A::add(dx[e], dy[e]), dz[e]));
+							}
 						}
 					}
 					const int Y = Y0 + v;
@@ -664,11 +713,19 @@ template <typename S, int R> struct Shape<S, R, 1> {
 template <typename S, int R> struct Shape<S, R, 2> {   // 9 warps; two CTAs per SM for R <= 4
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = 16, VY = 1, PF = 2, MINB = R <= 4 ? 2 : 1; };
 
+// Shared memory a CTA may use on sm_100 (227 KB).
+constexpr int kMaxSmemPerBlock = 232448;
+
 template <typename S, int R, int MODE, int SHAPE, bool EXACT>
 int launch_shape(const ZLaunch& L)
 {
 	using Sh = Shape<S, R, SHAPE>;
-	return launch_zmarch<ZCfg<S, R, MODE, Sh::TX, Sh::TY, Sh::VY, Sh::PF, EXACT, Sh::MINB>>(L);
+	using Cfg = ZCfg<S, R, MODE, Sh::TX, Sh::TY, Sh::VY, Sh::PF, EXACT, Sh::MINB>;
+	if constexpr (Cfg::SMEM > kMaxSmemPerBlock)
+		return set_error(B200_ERR_UNSUPPORTED, "stencil shape %d needs %d bytes of shared memory",
+				SHAPE, Cfg::SMEM);
+	else
+		return launch_zmarch<Cfg>(L);
 }
 
 // Dispatch storage type, half width, shape and arithmetic for one operator. NSHAPES and
