@@ -81,6 +81,7 @@ SIGNATURES = {
     "b200_max_err": [_PL, Field, Field, _PB, _D, _PD, _VP],
     "b200_min_max": [_PL, Field, _PB, _PD, _PD, _VP],
     "b200_l1_sums_separable": [_PL, Field, _PB, _VP, _VP, _VP, _D, _I, _PD, _PD, _VP],
+    "b200_l1_sums_separable_noalloc": [_PL, Field, _PB, _VP, _VP, _VP, _D, _I, _PD, _PD, _VP],
     "b200_device_status": [ctypes.POINTER(_I), _I],
     "b200_stencil_route": [_PL, _I, _I, ctypes.POINTER(_I)],
     "b200_set_arith_mode": [_I],

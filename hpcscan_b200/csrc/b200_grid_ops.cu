@@ -1,5 +1,7 @@
 // Grid operations of the hpcscan_b200 C ABI other than the stencils: fills, the
 // anti-mirror boundary condition, the split pressure update and the FP64 norms.
+#include <mutex>
+
 #include "b200_common.cuh"
 
 namespace b200 {
@@ -627,6 +629,121 @@ int b200_l1_sums_separable(const b200_layout* lay, b200_field u, const b200_box*
 	r.amp = amp;
 	r.ref_dtype = ref_dtype;
 	return run_reduce<RED_L1_SEP>(lay, u, nullptr, box, r, sum_abs_diff, sum_abs_ref, stream);
+}
+
+}  // extern "C"
+
+// ---- b200_l1_sums_separable_noalloc: the same norm on preallocated scratch ---------------------
+namespace b200 {
+namespace {
+constexpr int kNoAllocTableMax = 16384;    // table entries: nx + ny + nz of the box
+constexpr int kNoAllocPartialMax = 2048;   // stage-1 partial pairs
+constexpr int kNoAllocDevices = 64;
+}  // namespace
+
+// The tables (kNoAllocTableMax doubles), then the partial pairs, then the result pair: about
+// 160 KB per device, part of the library's device image, so that no call allocates.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocTableMax + 2 * kNoAllocPartialMax + 2];
+
+namespace {
+double* g_noalloc_ptr[kNoAllocDevices] = {};
+std::mutex g_noalloc_mutex;
+
+// Once per device, with that device current: the scratch's device address, and the kernels the
+// entry point launches loaded, so that later calls neither load nor allocate anything.
+int noalloc_scratch(double** out)
+{
+	int dev = 0;
+	if (int rc = cuda_error(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+	if (dev < 0 || dev >= kNoAllocDevices) return set_error(B200_ERR_ARG, "device index %d", dev);
+	std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+	if (!g_noalloc_ptr[dev]) {
+		void* p = nullptr;
+		if (int rc = cuda_error(cudaGetSymbolAddress(&p, g_noalloc_scratch),
+					"cudaGetSymbolAddress(no-alloc scratch)"))
+			return rc;
+		cudaFuncAttributes fa;
+		const void* kernels[] = {
+				reinterpret_cast<const void*>(k_reduce<float, RED_L1_SEP>),
+				reinterpret_cast<const void*>(k_reduce<double, RED_L1_SEP>),
+				reinterpret_cast<const void*>(k_reduce<__half, RED_L1_SEP>),
+				reinterpret_cast<const void*>(k_reduce<__nv_bfloat16, RED_L1_SEP>),
+				reinterpret_cast<const void*>(k_reduce_final<RED_L1_SEP>)};
+		for (const void* k : kernels)
+			if (int rc = cuda_error(cudaFuncGetAttributes(&fa, k), "cudaFuncGetAttributes(no-alloc)"))
+				return rc;
+		num_sms();
+		g_noalloc_ptr[dev] = static_cast<double*>(p);
+	}
+	*out = g_noalloc_ptr[dev];
+	return B200_OK;
+}
+}  // namespace
+}  // namespace b200
+
+extern "C" {
+
+int b200_l1_sums_separable_noalloc(const b200_layout* lay, b200_field u, const b200_box* box,
+		const double* v1, const double* v2, const double* v3, double amp, int ref_dtype,
+		double* sum_abs_diff, double* sum_abs_ref, void* stream)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_box(lay, box)) return rc;
+	if (int rc = check_field(u, "u")) return rc;
+	if (dtype_size(ref_dtype) == 0) return set_error(B200_ERR_ARG, "ref dtype %d", ref_dtype);
+	if (!v1 || !v2 || !v3) return set_error(B200_ERR_ARG, "NULL table");
+	const Box3 b = to_box3(box);
+	const int64_t entries = (int64_t)b.nx + b.ny + b.nz;
+	if (entries > kNoAllocTableMax)
+		return set_error(B200_ERR_UNSUPPORTED,
+				"b200_l1_sums_separable_noalloc: the box needs %lld table entries (nx + ny + nz), "
+				"its preallocated scratch holds %d; use b200_l1_sums_separable",
+				(long long)entries, kNoAllocTableMax);
+	double* scr = nullptr;
+	if (int rc = noalloc_scratch(&scr)) return rc;
+	double* t1 = scr;
+	double* t2 = t1 + b.nx;
+	double* t3 = t2 + b.ny;
+	double2* partial = reinterpret_cast<double2*>(scr + kNoAllocTableMax);
+	double2* result = partial + kNoAllocPartialMax;
+	cudaStream_t s = as_stream(stream);
+	int rc = cuda_error(cudaMemcpyAsync(t1, v1, b.nx * sizeof(double), cudaMemcpyHostToDevice, s), "tables");
+	if (!rc) rc = cuda_error(cudaMemcpyAsync(t2, v2, b.ny * sizeof(double), cudaMemcpyHostToDevice, s), "tables");
+	if (!rc) rc = cuda_error(cudaMemcpyAsync(t3, v3, b.nz * sizeof(double), cudaMemcpyHostToDevice, s), "tables");
+	if (rc) return rc;
+	RedArgs r{};
+	r.n1 = lay->n1;
+	r.n12 = lay->n1 * lay->n2;
+	r.b = b;
+	r.s1 = u.scale;
+	r.s2 = 1.0;
+	r.v1 = t1;
+	r.v2 = t2;
+	r.v3 = t3;
+	r.amp = amp;
+	r.ref_dtype = ref_dtype;
+	// the partition of the allocating entry point, so that both give the same sums
+	const int64_t rows = (int64_t)b.ny * b.nz;
+	int blocks = num_sms() * 8;
+	if (rows < blocks) blocks = (int)(rows > 0 ? rows : 1);
+	if (blocks > kNoAllocPartialMax) blocks = kNoAllocPartialMax;
+	rc = dispatch_dtype(u.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		k_reduce<S, RED_L1_SEP><<<blocks, kRedThreads, 0, s>>>(static_cast<const S*>(u.data),
+				nullptr, r, partial);
+		return check_launch("k_reduce(no-alloc)");
+	});
+	if (rc) return rc;
+	k_reduce_final<RED_L1_SEP><<<1, kRedThreads, 0, s>>>(partial, blocks, result);
+	if ((rc = check_launch("k_reduce_final(no-alloc)"))) return rc;
+	double2 v;
+	if ((rc = cuda_error(cudaMemcpyAsync(&v, result, sizeof(double2), cudaMemcpyDeviceToHost, s),
+				 "cudaMemcpyAsync(no-alloc norm)")))
+		return rc;
+	if ((rc = cuda_error(cudaStreamSynchronize(s), "cudaStreamSynchronize(no-alloc norm)"))) return rc;
+	if (sum_abs_diff) *sum_abs_diff = v.x;
+	if (sum_abs_ref) *sum_abs_ref = v.y;
+	return B200_OK;
 }
 
 }  // extern "C"

@@ -170,6 +170,23 @@ int b200_l1_sums_separable(const b200_layout* lay, b200_field u, const b200_box*
 		const double* v1, const double* v2, const double* v3, double amp, int ref_dtype,
 		double* sum_abs_diff, double* sum_abs_ref, void* stream);
 
+/* b200_l1_sums_separable without any allocation (no counterpart in the reference, whose CPU
+ * norms need no device memory). For callers that must not allocate once their time loop runs:
+ * an application whose own pool holds the device memory (a cudaMalloc could fail there), or one
+ * that cannot take the device-wide synchronisation of the cudaFree with which
+ * b200_l1_sums_separable grows its scratch, or the pinned host buffer it allocates for results.
+ * Works on a 160 KB scratch array compiled into the library, one per device: the tables of at
+ * most 16384 entries (box nx + ny + nz; larger boxes are rejected with B200_ERR_UNSUPPORTED)
+ * and at most 2048 partial sums. The first call on a device sets up (takes the array's device
+ * address and loads the kernels) and should precede any stream capture; later calls allocate
+ * and load nothing. Nothing in the scratch must start at zero: each call writes every entry it
+ * reads. The scratch is shared by all calls on a device, so calls that overlap (from two host
+ * threads, or on two streams) race; serialise them. Same results as b200_l1_sums_separable;
+ * synchronous on `stream`. */
+int b200_l1_sums_separable_noalloc(const b200_layout* lay, b200_field u, const b200_box* box,
+		const double* v1, const double* v2, const double* v3, double amp, int ref_dtype,
+		double* sum_abs_diff, double* sum_abs_ref, void* stream);
+
 /* ---- arithmetic mode and tuning ---------------------------------------------------------------
  * B200_ARITH_EXACT (default): every multiply and add of the stencil operators is a separately
  * rounded IEEE operation in the reference's evaluation order, so FP32/FP64 results are
