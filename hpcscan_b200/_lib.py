@@ -69,6 +69,7 @@ SIGNATURES = {
     "b200_copy_box_h2d": [_PL, _I, _VP, _VP, _PB, _VP],
     "b200_fill_const": [_PL, Field, _PB, _D, _VP],
     "b200_fill_separable": [_PL, Field, _PB, _VP, _VP, _VP, _D, _VP],
+    "b200_array_op": [_I, ctypes.c_int64, Field, Field, Field, _D, _VP],
     "b200_fd_d2": [_PL, _I, _I, Field, Field, _D, _D, _D, _VP],
     "b200_laplacian": [_PL, _I, Field, Field, _D, _D, _D, _VP],
     "b200_update_pressure": [_PL, Field, Field, Field, Field, _VP],
@@ -91,6 +92,7 @@ SIGNATURES = {
     "b200_autotune_stencil": [_PL, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), _PD],
 }
 B200_ARITH_EXACT, B200_ARITH_FMA = 0, 1
+B200_ARRAY_FILL, B200_ARRAY_COPY, B200_ARRAY_ADD, B200_ARRAY_MUL, B200_ARRAY_ADD_UPDATE = range(5)
 OP_FD_D2_N1, OP_FD_D2_N2, OP_FD_D2_N3, OP_LAPLACIAN, OP_PRESSURE, OP_STEP = 1, 2, 3, 4, 5, 6
 _RESTYPE = {"b200_last_error": ctypes.c_char_p}
 

@@ -61,6 +61,16 @@ template <> struct Storage<__nv_bfloat16> {
 	static __device__ __forceinline__ __nv_bfloat16 store_d(double v) { return __double2bfloat16(v); }
 };
 
+// A host-side double rounded once to the storage type (for kernel arguments).
+template <typename S>
+inline S host_store(double v)
+{
+	if constexpr (std::is_same_v<S, float>) return (float)v;
+	else if constexpr (std::is_same_v<S, double>) return v;
+	else if constexpr (std::is_same_v<S, __half>) return __double2half(v);
+	else return __double2bfloat16(v);
+}
+
 // ---- arithmetic with explicit rounding ---------------------------------------------------------
 // EXACT = true: every multiply and add is a separately rounded IEEE operation (no FMA
 // contraction), the order of the reference's CPU expressions compiled without FP

@@ -38,6 +38,28 @@ __global__ void k_fill_const(S* __restrict__ u, int64_t n1, int64_t n12, Box3 b,
 	u[i1 + i2 * n1 + i3 * n12] = val;
 }
 
+// Whole-array operations of the Memory test case (Grid::fillArray .. addUpdateArray).
+template <typename S, int OP>
+__global__ void k_array_op(S* __restrict__ out, const S* __restrict__ a, const S* __restrict__ b,
+		int64_t n, S val)
+{
+	using A = Arith<true>;
+	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+		if constexpr (OP == B200_ARRAY_FILL) {
+			out[i] = val;
+		} else if constexpr (OP == B200_ARRAY_COPY) {
+			out[i] = a[i];
+		} else if constexpr (OP == B200_ARRAY_ADD) {
+			out[i] = Storage<S>::store(A::add(Storage<S>::load(a[i]), Storage<S>::load(b[i])));
+		} else if constexpr (OP == B200_ARRAY_MUL) {
+			out[i] = Storage<S>::store(A::mul(Storage<S>::load(a[i]), Storage<S>::load(b[i])));
+		} else {
+			out[i] = Storage<S>::store(A::add(Storage<S>::load(out[i]), Storage<S>::load(a[i])));
+		}
+	}
+}
+
 template <typename S>
 __global__ void k_fill_separable(S* __restrict__ u, int64_t n1, int64_t n12, Box3 b,
 		const double* __restrict__ v1, const double* __restrict__ v2,
@@ -509,14 +531,50 @@ int b200_fill_const(const b200_layout* lay, b200_field u, const b200_box* box, d
 	const double v = val / (double)u.scale;
 	return dispatch_dtype(u.dtype, [&](auto tag) {
 		using S = decltype(tag);
-		S sv;
-		if constexpr (std::is_same_v<S, float>) sv = (float)v;
-		else if constexpr (std::is_same_v<S, double>) sv = v;
-		else if constexpr (std::is_same_v<S, __half>) sv = __double2half(v);
-		else sv = __double2bfloat16(v);
+		const S sv = host_store<S>(v);
 		k_fill_const<S><<<row_grid(b), kRowThreads, 0, as_stream(stream)>>>(
 				static_cast<S*>(u.data), lay->n1, lay->n1 * lay->n2, b, sv);
 		return check_launch("k_fill_const");
+	});
+}
+
+int b200_array_op(int op, int64_t n, b200_field out, b200_field in1, b200_field in2, double val,
+		void* stream)
+{
+	if (op < B200_ARRAY_FILL || op > B200_ARRAY_ADD_UPDATE)
+		return set_error(B200_ERR_ARG, "array operation %d", op);
+	if (n < 0) return set_error(B200_ERR_ARG, "array size %lld", (long long)n);
+	if (int rc = check_field(out, "out")) return rc;
+	const bool one = op == B200_ARRAY_COPY || op == B200_ARRAY_ADD_UPDATE;
+	const bool two = op == B200_ARRAY_ADD || op == B200_ARRAY_MUL;
+	if (one || two) {
+		if (int rc = check_field(in1, "in1")) return rc;
+		if (in1.dtype != out.dtype) return set_error(B200_ERR_UNSUPPORTED, "mixed storage types");
+	}
+	if (two) {
+		if (int rc = check_field(in2, "in2")) return rc;
+		if (in2.dtype != out.dtype) return set_error(B200_ERR_UNSUPPORTED, "mixed storage types");
+	}
+	if (op != B200_ARRAY_FILL && (out.scale != 1.0f || in1.scale != 1.0f || (two && in2.scale != 1.0f)))
+		return set_error(B200_ERR_UNSUPPORTED, "array operations on scaled fields");
+	if (n == 0) return B200_OK;
+	int blocks = num_sms() * 4;
+	if ((int64_t)blocks * kRowThreads > n) blocks = (int)((n + kRowThreads - 1) / kRowThreads);
+	cudaStream_t s = as_stream(stream);
+	return dispatch_dtype(out.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		S* o = static_cast<S*>(out.data);
+		const S* a = static_cast<const S*>(in1.data);
+		const S* b = static_cast<const S*>(in2.data);
+		const S v = host_store<S>(val / (double)out.scale);
+		switch (op) {
+		case B200_ARRAY_FILL: k_array_op<S, B200_ARRAY_FILL><<<blocks, kRowThreads, 0, s>>>(o, a, b, n, v); break;
+		case B200_ARRAY_COPY: k_array_op<S, B200_ARRAY_COPY><<<blocks, kRowThreads, 0, s>>>(o, a, b, n, v); break;
+		case B200_ARRAY_ADD: k_array_op<S, B200_ARRAY_ADD><<<blocks, kRowThreads, 0, s>>>(o, a, b, n, v); break;
+		case B200_ARRAY_MUL: k_array_op<S, B200_ARRAY_MUL><<<blocks, kRowThreads, 0, s>>>(o, a, b, n, v); break;
+		default: k_array_op<S, B200_ARRAY_ADD_UPDATE><<<blocks, kRowThreads, 0, s>>>(o, a, b, n, v); break;
+		}
+		return check_launch("k_array_op");
 	});
 }
 

@@ -120,6 +120,29 @@ class Grid:
         _lib.call("b200_fill_separable", ctypes.byref(lay), self.c_field(), ctypes.byref(box),
                   *ptrs, float(amp), _stream_ptr(stream))
 
+    # ---- whole-array operations (Grid::fillArray .. addUpdateArray, src/grid.cpp:1828-1918) ------
+    def _array_op(self, op: int, a: Optional["Grid"], b: Optional["Grid"], val: float,
+                  stream=None) -> None:
+        none = _lib.Field(None, self.c_field().dtype, 1.0)
+        _lib.call("b200_array_op", op, self.layout.npoint, self.c_field(),
+                  a.c_field() if a is not None else none, b.c_field() if b is not None else none,
+                  float(val), _stream_ptr(stream))
+
+    def fillArray(self, val: float, stream=None) -> None:
+        self._array_op(_lib.B200_ARRAY_FILL, None, None, val, stream)
+
+    def copyArray(self, gridIn: "Grid", stream=None) -> None:
+        self._array_op(_lib.B200_ARRAY_COPY, gridIn, None, 0.0, stream)
+
+    def addArray(self, gridIn1: "Grid", gridIn2: "Grid", stream=None) -> None:
+        self._array_op(_lib.B200_ARRAY_ADD, gridIn1, gridIn2, 0.0, stream)
+
+    def multiplyArray(self, gridIn1: "Grid", gridIn2: "Grid", stream=None) -> None:
+        self._array_op(_lib.B200_ARRAY_MUL, gridIn1, gridIn2, 0.0, stream)
+
+    def addUpdateArray(self, gridIn: "Grid", stream=None) -> None:
+        self._array_op(_lib.B200_ARRAY_ADD_UPDATE, gridIn, None, 0.0, stream)
+
     # ---- FD operators (`self` is the input, W the output; INNER points) --------------------------
     def _fd(self, axis: int, W: "Grid", order: int, name: str, stream=None) -> int:
         if not self.sameSize(W):

@@ -1,10 +1,10 @@
 /*
  * Single-rank stand-in for <mpi.h>, written for this project.
  *
- * Test infrastructure only: it lets the hpcscan reference CPU path
- * (src/*.cpp of the reference, compiled unchanged from where it lies) build
- * and run as ONE process without an MPI installation, so that it can serve
- * as the oracle and as the timed CPU baseline.
+ * It lets the hpcscan sources (src/*.cpp of the reference, compiled
+ * unchanged from where they lie) build and run as ONE process without an MPI
+ * installation: in the B200 test-mode binary (hpcscan_b200/host), and in the
+ * reference CPU build that the tests use as oracle and CPU baseline.
  *
  * Semantics for a world of size 1:
  *  - every neighbour is MPI_PROC_NULL (the reference computes that itself

@@ -106,6 +106,18 @@ int b200_fill_const(const b200_layout* lay, b200_field u, const b200_box* box, d
 int b200_fill_separable(const b200_layout* lay, b200_field u, const b200_box* box,
 		const double* v1, const double* v2, const double* v3, double amp, void* stream);
 
+/* Whole-array operations over n elements (every point, halos and padding included), the
+ * Memory test case's Grid::fillArray, copyArray, addArray, multiplyArray and addUpdateArray
+ * (src/grid.cpp:1828-1918), in the storage type's arithmetic. in2 is read by ADD and MUL
+ * only, in1 by all but FILL; fields must have scale 1 (FILL excepted). */
+#define B200_ARRAY_FILL       0   /* out = val        */
+#define B200_ARRAY_COPY       1   /* out = in1        */
+#define B200_ARRAY_ADD        2   /* out = in1 + in2  */
+#define B200_ARRAY_MUL        3   /* out = in1 * in2  */
+#define B200_ARRAY_ADD_UPDATE 4   /* out = out + in1  */
+int b200_array_op(int op, int64_t n, b200_field out, b200_field in1, b200_field in2, double val,
+		void* stream);
+
 /* ---- finite-difference operators (INNER points; `u` in, `w` out) ----------------------------
  * inv2_a = (1/d_a)^2 evaluated in the compute type by the caller (src/grid.cpp:3252-3258).
  * Grid::FD_D2_N1/N2/N3 (src/grid.cpp:3232, 3566, 3900); axis = 1, 2 or 3. */

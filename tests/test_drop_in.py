@@ -1,0 +1,112 @@
+"""hpcscan's own test cases, unchanged, on -testMode B200.
+
+hpcscan_b200/host/bin/hpcscan_b200_fp{32,64} are hpcscan's drivers (main, test cases,
+propagators, factories, the Grid base class) compiled from the hpcscan sources with Grid_B200
+registered in the factories. The same test case on the reference CPU build (oracle/_ref, modes
+Baseline / CacheBlk) is the yardstick: every "Test PASSED / ... err." line and the Propa
+errTestCase must agree.
+
+CPU tests check that the wrapped factories leave the CPU modes untouched; GPU tests run B200.
+"""
+import os
+import re
+import subprocess
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+B200_BIN = {p: os.path.join(REPO, "hpcscan_b200", "host", "bin", f"hpcscan_b200_{p}")
+            for p in ("fp32", "fp64")}
+REF_BIN = {p: os.path.join(REPO, "oracle", "_ref", f"hpcscan_{p}") for p in ("fp32", "fp64")}
+
+RESULT = re.compile(r"Test (PASSED|FAILED)!? / (\w+) err\.\s+(\S+)")
+PROPA_ERR = re.compile(r"errTestCase2\s+(\S+)")
+
+
+def run(binary, args, tmp_path):
+    if not os.path.exists(binary):
+        pytest.skip(f"{os.path.relpath(binary, REPO)} not built")
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "4"))
+    p = subprocess.run([binary] + args, cwd=tmp_path, capture_output=True, text=True, timeout=900,
+                       env=env)
+    assert p.returncode == 0, p.stdout[-3000:] + p.stderr[-3000:]
+    assert "TERMINATED SUCCESSFULLY" in p.stdout, p.stdout[-3000:]
+    assert "No test case was executed" not in p.stdout, p.stdout[-3000:]
+    return p.stdout
+
+
+def results(out):
+    return [(s, k, float(v)) for s, k, v in RESULT.findall(out)]
+
+
+def propa_err(out):
+    m = PROPA_ERR.findall(out)
+    assert m and "Test PASSED" in out, out[-3000:]
+    return float(m[-1])
+
+
+def same_results(got, want, rtol, atol):
+    assert len(got) == len(want) > 0, (got, want)
+    for (sg, kg, vg), (sw, kw, vw) in zip(got, want):
+        assert (sg, kg) == (sw, kw), (got, want)
+        assert abs(vg - vw) <= atol + rtol * abs(vw), (kg, vg, vw)
+
+
+GRID_ARGS = ["-n1", "40", "-n2", "40", "-n3", "40", "-ntry", "1"]
+
+
+# ---- CPU: the factory wrapping leaves the hpcscan CPU modes as they are ------------------------
+
+@pytest.mark.parametrize("case", ["Grid", "FD_D2", "Propa"])
+def test_cpu_modes_unchanged_by_b200_registration(tmp_path, case):
+    args = ["-testCase", case, "-testMode", "CacheBlk"] + GRID_ARGS
+    got = run(B200_BIN["fp32"], args, tmp_path)
+    want = run(REF_BIN["fp32"], args, tmp_path)
+    if case == "Propa":
+        assert propa_err(got) == propa_err(want)
+    else:
+        assert results(got) == results(want)
+
+
+# ---- GPU: the unchanged test cases on the B200 path ---------------------------------------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,order,propagator", [
+    ("fp32", 8, "Ac2Standard"), ("fp32", 2, "Ac2Standard"), ("fp32", 16, "Ac2Standard"),
+    ("fp32", 8, "Ac2SplitComp"), ("fp64", 8, "Ac2Standard"), ("fp64", 12, "Ac2SplitComp")])
+def test_propa_b200_equals_reference(tmp_path, prec, order, propagator):
+    """Eigen-mode propagation (TestCase_Propa) with the reference's check every step: the
+    errTestCase of B200 equals the reference CPU build's (wavefields are bit-identical; only the
+    FP64 summation order of the norms differs)."""
+    args = ["-testCase", "Propa", "-propagator", propagator, "-fdOrder", str(order),
+            "-n1", "70", "-n2", "61", "-n3", "53", "-ratioCFL", "0.8", "-nt", "60", "-ntry", "1"]
+    got = propa_err(run(B200_BIN[prec], args + ["-testMode", "B200"], tmp_path))
+    want = propa_err(run(REF_BIN[prec], args + ["-testMode", "Baseline"], tmp_path))
+    assert abs(got - want) <= 1e-5 * abs(want), (got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("order", [2, 4, 6, 8, 10, 12, 14, 16])
+def test_fd_d2_b200_equals_reference(tmp_path, prec, order):
+    """TestCase_FD_D2: D2 along each axis and the Laplacian of sin(a1 x1) sin(a2 x2) sin(a3 x3)
+    against the analytic derivatives; the same L1 errors and verdicts as the reference CPU
+    build (at this size O2 misses the 1e-3 threshold on both)."""
+    args = ["-testCase", "FD_D2", "-fdOrder", str(order), "-n1", "50", "-n2", "44", "-n3", "38",
+            "-param1", "4", "-param2", "6", "-param3", "8", "-param4", "1", "-ntry", "1"]
+    got = results(run(B200_BIN[prec], args + ["-testMode", "B200"], tmp_path))
+    want = results(run(REF_BIN[prec], args + ["-testMode", "Baseline"], tmp_path))
+    same_results(got, want, rtol=1e-5, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["Grid", "Memory"])
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_grid_and_memory_cases_pass_on_b200(tmp_path, case, prec):
+    """TestCase_Grid (fill, norms, min/max, updatePressure, boundary condition) and
+    TestCase_Memory (whole-array operations): every check passes on B200, with the reference's
+    tolerance, and reports what the reference CPU build reports."""
+    args = ["-testCase", case] + GRID_ARGS
+    got = results(run(B200_BIN[prec], args + ["-testMode", "B200"], tmp_path))
+    want = results(run(REF_BIN[prec], args + ["-testMode", "Baseline"], tmp_path))
+    same_results(got, want, rtol=1e-4, atol=1e-6)

@@ -148,6 +148,26 @@ def test_update_pressure_bitexact(gpu, oracle, lay):
     assert np.array_equal(bits(G[0].to_numpy()), bits(ref))
 
 
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_array_ops_bitexact(gpu, prec):
+    """Grid::fillArray / copyArray / addArray / multiplyArray / addUpdateArray over every point
+    (src/grid.cpp:1828-1918): IEEE operations in the storage type, so numpy gives the bits."""
+    lay = L.b200_layout(3, 30, 21, 22, order=4, prec=prec)
+    t = np.float32 if prec == "f32" else np.float64
+    a, b, c = rand_field(lay, 21), rand_field(lay, 22), rand_field(lay, 23)
+    A, B, C, W = dev(lay, a), dev(lay, b), dev(lay, c), dev(lay)
+    W.fillArray(0.3)
+    assert np.array_equal(bits(W.to_numpy()), bits(np.full(lay.npoint, 0.3, dtype=t)))
+    W.copyArray(A)
+    assert np.array_equal(bits(W.to_numpy()), bits(a))
+    W.addArray(A, B)
+    assert np.array_equal(bits(W.to_numpy()), bits(a + b))
+    W.multiplyArray(A, B)
+    assert np.array_equal(bits(W.to_numpy()), bits(a * b))
+    W.addUpdateArray(C)
+    assert np.array_equal(bits(W.to_numpy()), bits(a * b + c))
+
+
 BC_LAYOUTS = [L.b200_layout(3, 30, 21, 22, order=8), L.reference_layout(3, 25, 20, 21, order=16),
               L.b200_layout(3, 12, 9, 10, order=16, prec="f64"),      # small: sequential faces
               L.reference_layout(2, 33, 20, order=4, prec="f64"), L.reference_layout(1, 40, order=6)]
