@@ -69,19 +69,16 @@ std::mutex g_tune_mutex;
 int g_arith = B200_ARITH_EXACT;
 
 // Untuned defaults: the fastest shape measured at 512^3 on B200 for each storage type and
-// half width (FP32: two-row 28x64 tiles up to R = 2, 14x64 tiles with 128-plane chunks for
-// R = 3..4, 9-warp 16x64 tiles beyond, where the 30-row tiles run out of registers; FP64:
-// 14x32 tiles, 30x32 tiles for R = 5..7; at R = 8 those exceed the shared memory).
+// half width (FP32: two-row 28x64 tiles up to R = 2, 14x64 tiles for R = 3..4, 9-warp 16x64
+// tiles beyond, where the 30-row tiles run out of registers; FP64: 14x32 tiles, 30x32 tiles for
+// R = 5..7; at R = 8 those exceed the shared memory). The z-chunk follows the grid size
+// (pick_nz_chunk).
 Tuned default_tuning(int dtype, int R)
 {
 	Tuned t;
-	if (dtype == B200_F64) {
-		t.shape = (R <= 4 || R == 8) ? 0 : 1;
-		t.nz_chunk = R > 4 ? 128 : 0;
-	} else {
-		t.shape = R <= 4 ? 0 : 2;
-		t.nz_chunk = (R >= 3 && R <= 4) ? 128 : 0;
-	}
+	if (dtype == B200_F64) t.shape = (R <= 4 || R == 8) ? 0 : 1;
+	else t.shape = R <= 4 ? 0 : 2;
+	t.nz_chunk = 0;
 	return t;
 }
 

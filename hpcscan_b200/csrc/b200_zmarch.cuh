@@ -639,7 +639,8 @@ int make_map(CUtensorMap* m, const void* base, int dtype, const b200_layout* lay
 
 namespace {
 
-// planes per CTA: enough CTAs for several waves, long enough chunks to amortise the z-halo
+// planes per CTA: long chunks amortise the z-halo (2R planes per chunk), as long as the grid
+// still fills the GPU twice over with resident CTAs (64 planes for R <= 2, 128 beyond, at 512^3)
 template <class Cfg>
 int pick_nz_chunk(int ntiles, int nz, int requested)
 {
@@ -648,8 +649,8 @@ int pick_nz_chunk(int ntiles, int nz, int requested)
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zmarch<Cfg>, Cfg::NT, Cfg::SMEM);
 	if (per_sm < 1) per_sm = 1;
 	const int resident = per_sm * num_sms();
-	int chunk = Cfg::R <= 4 ? 64 : 128;
-	while (chunk > 16 && (int64_t)ntiles * ((nz + chunk - 1) / chunk) < 4 * (int64_t)resident) chunk /= 2;
+	int chunk = Cfg::R <= 2 ? 64 : 128;
+	while (chunk > 16 && (int64_t)ntiles * ((nz + chunk - 1) / chunk) < 2 * (int64_t)resident) chunk /= 2;
 	return chunk < nz ? chunk : nz;
 }
 
@@ -708,8 +709,8 @@ int launch_zmarch(const ZLaunch& L)
 template <typename S, int R, int SHAPE> struct Shape;
 template <typename S, int R> struct Shape<S, R, 0> {
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 2, MINB = 0; };
-template <typename S, int R> struct Shape<S, R, 1> {
-	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = 30, VY = 1, PF = 2, MINB = 0; };
+template <typename S, int R> struct Shape<S, R, 1> {   // shape 0 with a deeper prefetch ring
+	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 4, MINB = 0; };
 template <typename S, int R> struct Shape<S, R, 2> {   // 9 warps; two CTAs per SM for R <= 4
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = 16, VY = 1, PF = 2, MINB = R <= 4 ? 2 : 1; };
 
