@@ -295,11 +295,15 @@ def b200_arm(a):
     peak, peak_src = measured_peak()
     achieved = ALG_BYTES_PER_POINT * pts / (kmean * 1e-3) / 1e9
     traffic = profiled_traffic()
+    if traffic is not None and (traffic.get("workload", {}).get("n") != a.size or
+                                traffic.get("workload", {}).get("order") != a.order):
+        traffic = None          # the committed capture covers another workload
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_src,
             "kernel": KERNEL_NAME, "kernel_ms": round(kmean, 5),
             "alg_bytes_per_point": ALG_BYTES_PER_POINT, "points_per_launch": pts,
-            "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch_scaled"),
+            "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
+            "traffic_unit": "bytes per launch",
             "traffic_note": None if traffic is None else traffic.get("note")}
     # free the timed grids before the end-to-end job
     del propa, prn, prc
