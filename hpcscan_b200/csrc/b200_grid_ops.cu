@@ -21,21 +21,30 @@ Box3 to_box3(const b200_box* b)
 			(int)(b->i3e - b->i3s + 1)};
 }
 
-dim3 row_grid(const Box3& b)
+// Row walk: the blocks of a grid take the rows (i2, i3) of a box, kUnroll rows at a time, and
+// the threads of a block stride along i1 (coalesced). A grid of at most 8 blocks per SM, each
+// thread with kUnroll independent loads in flight per step.
+constexpr int kRowUnroll = 4;
+
+int row_blocks(const Box3& b, int unroll)
 {
-	// blocks: x over i1 chunks, y over i2, z over i3 (grid.y/z limit 65535 — grids here are far
-	// smaller per axis)
-	return dim3((unsigned)((b.nx + kRowThreads - 1) / kRowThreads), (unsigned)b.ny, (unsigned)b.nz);
+	const int64_t rows = (int64_t)b.ny * b.nz;
+	const int64_t want = (rows + unroll - 1) / unroll;
+	const int64_t cap = (int64_t)num_sms() * 8;
+	return (int)(want < 1 ? 1 : (want < cap ? want : cap));
 }
 
 // ---- fills ------------------------------------------------------------------------------------
 template <typename S>
-__global__ void k_fill_const(S* __restrict__ u, int64_t n1, int64_t n12, Box3 b, S val)
+__global__ void __launch_bounds__(kRowThreads) k_fill_const(S* __restrict__ u, int64_t n1,
+		int64_t n12, Box3 b, S val)
 {
-	const int x = blockIdx.x * blockDim.x + threadIdx.x;
-	if (x >= b.nx) return;
-	const int64_t i1 = b.i1s + x, i2 = b.i2s + blockIdx.y, i3 = b.i3s + blockIdx.z;
-	u[i1 + i2 * n1 + i3 * n12] = val;
+	const int64_t rows = (int64_t)b.ny * b.nz;
+	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+		const int64_t y = row % b.ny, z = row / b.ny;
+		S* dst = u + b.i1s + (b.i2s + y) * n1 + (b.i3s + z) * n12;
+		for (int x = threadIdx.x; x < b.nx; x += blockDim.x) dst[x] = val;
+	}
 }
 
 // Whole-array operations of the Memory test case (Grid::fillArray .. addUpdateArray).
@@ -61,16 +70,19 @@ __global__ void k_array_op(S* __restrict__ out, const S* __restrict__ a, const S
 }
 
 template <typename S>
-__global__ void k_fill_separable(S* __restrict__ u, int64_t n1, int64_t n12, Box3 b,
-		const double* __restrict__ v1, const double* __restrict__ v2,
+__global__ void __launch_bounds__(kRowThreads) k_fill_separable(S* __restrict__ u, int64_t n1,
+		int64_t n12, Box3 b, const double* __restrict__ v1, const double* __restrict__ v2,
 		const double* __restrict__ v3, double amp)
 {
-	const int x = blockIdx.x * blockDim.x + threadIdx.x;
-	if (x >= b.nx) return;
-	const int y = blockIdx.y, z = blockIdx.z;
-	// (((amp * v1) * v2) * v3), each product rounded in FP64, then one rounding to S
-	const double v = __dmul_rn(__dmul_rn(__dmul_rn(amp, v1[x]), v2[y]), v3[z]);
-	u[(b.i1s + x) + (b.i2s + y) * n1 + (b.i3s + z) * n12] = Storage<S>::store_d(v);
+	const int64_t rows = (int64_t)b.ny * b.nz;
+	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+		const int y = (int)(row % b.ny), z = (int)(row / b.ny);
+		const double w2 = v2[y], w3 = v3[z];
+		S* dst = u + b.i1s + (b.i2s + y) * n1 + (b.i3s + z) * n12;
+		// (((amp * v1) * v2) * v3), each product rounded in FP64, then one rounding to S
+		for (int x = threadIdx.x; x < b.nx; x += blockDim.x)
+			dst[x] = Storage<S>::store_d(__dmul_rn(__dmul_rn(__dmul_rn(amp, v1[x]), w2), w3));
+	}
 }
 
 // ---- boundary condition ----------------------------------------------------------------------
@@ -87,43 +99,46 @@ struct BcArgs {
 // Valid when every used axis has at least halo + 2 inner points (checked by the caller).
 //
 // Block partition (kBcThreads threads per block, every index decoded once per block):
-//   [0, nbx)            x faces: 16 rows (i2, i3) per block, 16 lanes per row = (side, k)
-//   [nbx, nbx+nby)      y faces: one run of up to kBcThreads i1 values per (i3, side, k)
-//   [nbx+nby, +nbz)     z faces: one run of up to kBcThreads i1 values per (i2, side, k)
+//   [0, nbx)            x faces: L = 2 halo lanes (side, k) per row (i2, i3), kBcThreads / L
+//                       rows per block (L = 2 for the boundary planes)
+//   [nbx, nbx+nby)      y faces: one run of up to kBcThreads i1 values per (i3, side), all k
+//   [nbx+nby, +nbz)     z faces: one run of up to kBcThreads i1 values per (i2, side), all k
 constexpr int kBcThreads = 256;
 
 struct BcPart {
 	int nbx, nby, nbz;     // blocks per group
 	int nchunk;            // i1 runs per row for y/z groups
+	int lanes;             // x faces: lanes per row
 };
 
 BcPart bc_partition(const BcArgs& a, bool planes)
 {
 	const int nx = (int)(a.e[0] - a.s[0] + 1), ny = (int)(a.e[1] - a.s[1] + 1),
 	          nz = (int)(a.e[2] - a.s[2] + 1);
-	const int kk = planes ? 1 : a.halo;     // planes: only k = 0 (the boundary plane itself)
 	BcPart p;
+	p.lanes = planes ? 2 : 2 * a.halo;
 	p.nchunk = (nx + kBcThreads - 1) / kBcThreads;
-	const int rows_per_block = kBcThreads / 16;
+	const int rows_per_block = kBcThreads / p.lanes;
 	p.nbx = (ny * nz + rows_per_block - 1) / rows_per_block;
-	p.nby = a.dim >= 2 ? p.nchunk * nz * 2 * kk : 0;
-	p.nbz = a.dim >= 3 ? p.nchunk * ny * 2 * kk : 0;
+	p.nby = a.dim >= 2 ? p.nchunk * nz * 2 : 0;
+	p.nbz = a.dim >= 3 ? p.nchunk * ny * 2 : 0;
 	return p;
 }
 
 template <typename S>
 __global__ void __launch_bounds__(kBcThreads) k_bc_halos(S* __restrict__ u, BcArgs a, BcPart p)
 {
+	constexpr int KMAX = 8;
 	const int R = a.halo;
 	const int ny = (int)(a.e[1] - a.s[1] + 1);
 	const bool lo_x = a.faces & 1, hi_x = a.faces & 2, lo_y = a.faces & 4, hi_y = a.faces & 8;
 	int b = blockIdx.x;
 	if (b < p.nbx) {
-		const int lane = threadIdx.x & 15;
-		if (lane >= 2 * R) return;
+		const int lane = threadIdx.x % p.lanes, rib = threadIdx.x / p.lanes;
+		if (rib >= kBcThreads / p.lanes) return;
 		const int side = lane / R, k = lane % R + 1;
 		if (!(a.faces & (1 << side))) return;
-		const int row = b * (kBcThreads / 16) + (threadIdx.x >> 4);
+		const int row = b * (kBcThreads / p.lanes) + rib;
 		const int nrow = ny * (int)(a.e[2] - a.s[2] + 1);
 		if (row >= nrow) return;
 		const int64_t base = (a.s[1] + row % ny) * a.n1 + (a.s[2] + row / ny) * a.n12;
@@ -135,44 +150,52 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_halos(S* __restrict__ u, BcAr
 	const int axis = (b < p.nby) ? 1 : 2;
 	if (axis == 2) b -= p.nby;
 	const int chunk = b % p.nchunk;
-	int r = b / p.nchunk;
-	const int ks = r % (2 * R);
-	r /= 2 * R;                                  // i3 (y faces) or i2 (z faces), inner offset
-	const int side = ks / R, k = ks % R + 1;
+	const int r = b / p.nchunk;
+	const int side = r % 2;
+	const int line = r / 2;                      // i3 (y faces) or i2 (z faces), inner offset
 	const int x = chunk * kBcThreads + threadIdx.x;
 	if (a.s[0] + x > a.e[0]) return;
 	const int64_t i1 = a.s[0] + x;
+	S mv[KMAX];
 	if (axis == 1) {
 		if (!(a.faces & (4 << side))) return;
-		const int64_t i3 = a.s[2] + r;
-		const int64_t h = side ? a.e[1] + k : a.s[1] - k, m = side ? a.e[1] - k : a.s[1] + k;
+		const int64_t i3 = a.s[2] + line;
 		const bool zero = (lo_x && i1 == a.s[0]) || (hi_x && i1 == a.e[0]);
-		const S mv = zero ? S(0.0f) : u[i1 + m * a.n1 + i3 * a.n12];
-		u[i1 + h * a.n1 + i3 * a.n12] = Storage<S>::store(-Storage<S>::load(mv));
+		const int64_t col = i1 + i3 * a.n12;
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R) mv[k - 1] = zero ? S(0.0f) : u[col + (side ? a.e[1] - k : a.s[1] + k) * a.n1];
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R)
+				u[col + (side ? a.e[1] + k : a.s[1] - k) * a.n1] = Storage<S>::store(-Storage<S>::load(mv[k - 1]));
 	} else {
 		if (!(a.faces & (16 << side))) return;
-		const int64_t i2 = a.s[1] + r;
-		const int64_t h = side ? a.e[2] + k : a.s[2] - k, m = side ? a.e[2] - k : a.s[2] + k;
+		const int64_t i2 = a.s[1] + line;
 		const bool zero = (lo_x && i1 == a.s[0]) || (hi_x && i1 == a.e[0]) ||
 		                  (lo_y && i2 == a.s[1]) || (hi_y && i2 == a.e[1]);
-		const S mv = zero ? S(0.0f) : u[i1 + i2 * a.n1 + m * a.n12];
-		u[i1 + i2 * a.n1 + h * a.n12] = Storage<S>::store(-Storage<S>::load(mv));
+		const int64_t col = i1 + i2 * a.n1;
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R) mv[k - 1] = zero ? S(0.0f) : u[col + (side ? a.e[2] - k : a.s[2] + k) * a.n12];
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R)
+				u[col + (side ? a.e[2] + k : a.s[2] - k) * a.n12] = Storage<S>::store(-Storage<S>::load(mv[k - 1]));
 	}
 }
 
 // Phase B: the boundary planes (first/last inner point of each active face) set to zero,
-// same block partition with k = 0.
+// same block partition with one lane per side for the x faces.
 template <typename S>
 __global__ void __launch_bounds__(kBcThreads) k_bc_planes(S* __restrict__ u, BcArgs a, BcPart p)
 {
 	const int ny = (int)(a.e[1] - a.s[1] + 1);
 	int b = blockIdx.x;
 	if (b < p.nbx) {
-		const int lane = threadIdx.x & 15;
-		if (lane >= 2) return;
-		const int side = lane;
+		const int side = threadIdx.x % 2;
 		if (!(a.faces & (1 << side))) return;
-		const int row = b * (kBcThreads / 16) + (threadIdx.x >> 4);
+		const int row = b * (kBcThreads / 2) + threadIdx.x / 2;
 		const int nrow = ny * (int)(a.e[2] - a.s[2] + 1);
 		if (row >= nrow) return;
 		const int64_t base = (a.s[1] + row % ny) * a.n1 + (a.s[2] + row / ny) * a.n12;
@@ -231,18 +254,34 @@ __global__ void k_bc_face(S* __restrict__ u, BcArgs a, int face)
 
 // ---- split update ------------------------------------------------------------------------------
 template <typename S, bool EXACT>
-__global__ void k_update_pressure(S* __restrict__ prn, const S* __restrict__ prc,
-		const S* __restrict__ coef, const S* __restrict__ lapla, int64_t n1, int64_t n12, Box3 b,
-		float coef_scale)
+__global__ void __launch_bounds__(kRowThreads) k_update_pressure(S* __restrict__ prn,
+		const S* __restrict__ prc, const S* __restrict__ coef, const S* __restrict__ lapla,
+		int64_t n1, int64_t n12, Box3 b, float coef_scale)
 {
 	using C = typename Storage<S>::C;
-	const int x = blockIdx.x * blockDim.x + threadIdx.x;
-	if (x >= b.nx) return;
-	const int64_t ii = (b.i1s + x) + (b.i2s + blockIdx.y) * n1 + (b.i3s + blockIdx.z) * n12;
-	C c = Storage<S>::load(coef[ii]);
-	if (coef_scale != 1.0f) c = c * (C)coef_scale;
-	prn[ii] = Storage<S>::store(leapfrog<C, EXACT>(Storage<S>::load(prc[ii]),
-			Storage<S>::load(prn[ii]), c, Storage<S>::load(lapla[ii])));
+	const int64_t rows = (int64_t)b.ny * b.nz;
+	for (int64_t r0 = (int64_t)blockIdx.x * kRowUnroll; r0 < rows; r0 += (int64_t)gridDim.x * kRowUnroll) {
+		for (int x = threadIdx.x; x < b.nx; x += blockDim.x) {
+			int64_t ii[kRowUnroll];
+			C pc[kRowUnroll], pn[kRowUnroll], cf[kRowUnroll], lp[kRowUnroll];
+#pragma unroll
+			for (int k = 0; k < kRowUnroll; k++) {
+				const int64_t row = r0 + k < rows ? r0 + k : rows - 1;
+				ii[k] = (b.i1s + x) + (b.i2s + row % b.ny) * n1 + (b.i3s + row / b.ny) * n12;
+				pc[k] = Storage<S>::load(prc[ii[k]]);
+				pn[k] = Storage<S>::load(prn[ii[k]]);
+				cf[k] = Storage<S>::load(coef[ii[k]]);
+				lp[k] = Storage<S>::load(lapla[ii[k]]);
+			}
+#pragma unroll
+			for (int k = 0; k < kRowUnroll; k++) {
+				if (r0 + k >= rows) break;
+				C c = cf[k];
+				if (coef_scale != 1.0f) c = c * (C)coef_scale;
+				prn[ii[k]] = Storage<S>::store(leapfrog<C, EXACT>(pc[k], pn[k], c, lp[k]));
+			}
+		}
+	}
 }
 
 // ---- reductions -------------------------------------------------------------------------------
@@ -325,37 +364,56 @@ __device__ __forceinline__ double ref_value(const RedArgs& r, int x, int y, int 
 	}
 }
 
-// Stage 1: one partial (pair) per block; blocks stride over the rows (i2, i3) of the box,
-// threads along i1, so every read is coalesced. Deterministic for a given grid size.
+// Stage 1: one partial (pair) per block; the blocks walk the rows (i2, i3) of the box
+// kRowUnroll at a time, threads along i1 (coalesced, kRowUnroll loads in flight per thread).
+// Deterministic for a given grid size.
 template <typename S, int OP>
 __global__ void __launch_bounds__(kRedThreads) k_reduce(const S* __restrict__ u1,
 		const S* __restrict__ u2, RedArgs r, double2* __restrict__ partial)
 {
+	constexpr bool TWO = (OP == RED_L1 || OP == RED_MAX_ERR);
 	double a = (OP == RED_MAX_ERR) ? -(double)3.402823466e+38f : (OP == RED_MIN_MAX ? 1.0e308 : 0.0);
 	double b = (OP == RED_MIN_MAX) ? -1.0e308 : 0.0;
 	const int64_t rows = (int64_t)r.b.ny * r.b.nz;
-	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
-		const int y = (int)(row % r.b.ny), z = (int)(row / r.b.ny);
-		const int64_t base = r.b.i1s + (r.b.i2s + y) * r.n1 + (r.b.i3s + z) * r.n12;
+	for (int64_t r0 = (int64_t)blockIdx.x * kRowUnroll; r0 < rows; r0 += (int64_t)gridDim.x * kRowUnroll) {
+		int yk[kRowUnroll], zk[kRowUnroll];
+		int64_t base[kRowUnroll];
+#pragma unroll
+		for (int k = 0; k < kRowUnroll; k++) {
+			const int64_t row = r0 + k < rows ? r0 + k : rows - 1;
+			yk[k] = (int)(row % r.b.ny);
+			zk[k] = (int)(row / r.b.ny);
+			base[k] = r.b.i1s + (r.b.i2s + yk[k]) * r.n1 + (r.b.i3s + zk[k]) * r.n12;
+		}
 		for (int x = threadIdx.x; x < r.b.nx; x += blockDim.x) {
-			const double v1 = (double)Storage<S>::load(u1[base + x]) * r.s1;
-			if (OP == RED_SUM_ABS) {
-				a += fabs(v1);
-			} else if (OP == RED_MIN_MAX) {
-				a = fmin(a, v1);
-				b = fmax(b, v1);
-			} else {
-				double v2;
-				if (OP == RED_L1_SEP) v2 = ref_value<S>(r, x, y, z);
-				else v2 = (double)Storage<S>::load(u2[base + x]) * r.s2;
-				if (OP == RED_L1 || OP == RED_L1_SEP) {
-					a += fabs(v1 - v2);
-					b += fabs(v2);
-				} else {   // RED_MAX_ERR (src/grid.cpp:2031-2043)
-					double e;
-					if (fabsf((float)v2) < (float)r.max_err_float) e = fabs(v1 - v2);
-					else e = fabs(v1 - v2) / fabs(v2);
-					a = fmax(a, e);
+			double w1[kRowUnroll], w2[kRowUnroll];
+#pragma unroll
+			for (int k = 0; k < kRowUnroll; k++) {
+				w1[k] = (double)Storage<S>::load(u1[base[k] + x]) * r.s1;
+				if constexpr (TWO) w2[k] = (double)Storage<S>::load(u2[base[k] + x]) * r.s2;
+			}
+#pragma unroll
+			for (int k = 0; k < kRowUnroll; k++) {
+				if (r0 + k >= rows) break;
+				const double v1 = w1[k];
+				if constexpr (OP == RED_SUM_ABS) {
+					a += fabs(v1);
+				} else if constexpr (OP == RED_MIN_MAX) {
+					a = fmin(a, v1);
+					b = fmax(b, v1);
+				} else {
+					double v2;
+					if constexpr (OP == RED_L1_SEP) v2 = ref_value<S>(r, x, yk[k], zk[k]);
+					else v2 = w2[k];
+					if constexpr (OP == RED_L1 || OP == RED_L1_SEP) {
+						a += fabs(v1 - v2);
+						b += fabs(v2);
+					} else {   // RED_MAX_ERR (src/grid.cpp:2031-2043)
+						double e;
+						if (fabsf((float)v2) < (float)r.max_err_float) e = fabs(v1 - v2);
+						else e = fabs(v1 - v2) / fabs(v2);
+						a = fmax(a, e);
+					}
 				}
 			}
 		}
@@ -403,9 +461,7 @@ int run_reduce(const b200_layout* lay, const b200_field& u1, const b200_field* u
 	r.b = to_box3(box);
 	r.s1 = u1.scale;
 	r.s2 = u2 ? u2->scale : 1.0;
-	const int64_t rows = (int64_t)r.b.ny * r.b.nz;
-	int blocks = num_sms() * 8;
-	if (rows < blocks) blocks = (int)(rows > 0 ? rows : 1);
+	const int blocks = row_blocks(r.b, kRowUnroll);
 	void* scr;
 	if (int rc = scratch(sizeof(double2) * (blocks + 1), &scr)) return rc;
 	double2* partial = reinterpret_cast<double2*>(scr);
@@ -532,7 +588,7 @@ int b200_fill_const(const b200_layout* lay, b200_field u, const b200_box* box, d
 	return dispatch_dtype(u.dtype, [&](auto tag) {
 		using S = decltype(tag);
 		const S sv = host_store<S>(v);
-		k_fill_const<S><<<row_grid(b), kRowThreads, 0, as_stream(stream)>>>(
+		k_fill_const<S><<<row_blocks(b, 1), kRowThreads, 0, as_stream(stream)>>>(
 				static_cast<S*>(u.data), lay->n1, lay->n1 * lay->n2, b, sv);
 		return check_launch("k_fill_const");
 	});
@@ -591,7 +647,7 @@ int b200_fill_separable(const b200_layout* lay, b200_field u, const b200_box* bo
 	const double a = amp / (double)u.scale;
 	int rc = dispatch_dtype(u.dtype, [&](auto tag) {
 		using S = decltype(tag);
-		k_fill_separable<S><<<row_grid(b), kRowThreads, 0, s>>>(static_cast<S*>(u.data), lay->n1,
+		k_fill_separable<S><<<row_blocks(b, 1), kRowThreads, 0, s>>>(static_cast<S*>(u.data), lay->n1,
 				lay->n1 * lay->n2, b, d1, d2, d3, a);
 		return check_launch("k_fill_separable");
 	});
@@ -623,7 +679,7 @@ int b200_update_pressure(const b200_layout* lay, b200_field prn, b200_field prc,
 	const Box3 b = to_box3(&box);
 	return dispatch_dtype(prn.dtype, [&](auto tag) {
 		using S = decltype(tag);
-		k_update_pressure<S, true><<<row_grid(b), kRowThreads, 0, as_stream(stream)>>>(
+		k_update_pressure<S, true><<<row_blocks(b, kRowUnroll), kRowThreads, 0, as_stream(stream)>>>(
 				static_cast<S*>(prn.data), static_cast<const S*>(prc.data),
 				static_cast<const S*>(coef.data), static_cast<const S*>(lapla.data), lay->n1,
 				lay->n1 * lay->n2, b, coef.scale);
@@ -781,9 +837,7 @@ int b200_l1_sums_separable_noalloc(const b200_layout* lay, b200_field u, const b
 	r.amp = amp;
 	r.ref_dtype = ref_dtype;
 	// the partition of the allocating entry point, so that both give the same sums
-	const int64_t rows = (int64_t)b.ny * b.nz;
-	int blocks = num_sms() * 8;
-	if (rows < blocks) blocks = (int)(rows > 0 ? rows : 1);
+	int blocks = row_blocks(b, kRowUnroll);
 	if (blocks > kNoAllocPartialMax) blocks = kNoAllocPartialMax;
 	rc = dispatch_dtype(u.dtype, [&](auto tag) {
 		using S = decltype(tag);
