@@ -66,6 +66,22 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(dist, values, device):
+    """Per-rank timings -> their maxima over all ranks (one all-reduce that every rank takes);
+    the values themselves on a single process."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_gpoints(world, points_per_rank, steps, seconds):
+    """Whole-job throughput of `world` replicas, each updating points_per_rank x steps."""
+    return world * points_per_rank * steps / seconds / 1e9
+
+
 def measured_peak():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -281,14 +297,9 @@ def b200_arm(a):
     _lib.call("b200_device_status", ctypes.byref(st), 1)
     if st.value:
         raise RuntimeError(f"device-side error word {st.value}")
-    if dist is not None:
-        t = torch.tensor([ms, statistics.mean(kern_ms)], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, kmean = t.tolist()
-    else:
-        kmean = statistics.mean(kern_ms)
+    ms, kmean = max_over_ranks(dist, [ms, statistics.mean(kern_ms)], "cuda")
     pts = lay.inner_points
-    value = world * pts * a.steps / (ms * 1e-3) / 1e9
+    value = job_gpoints(world, pts, a.steps, ms * 1e-3)
 
     # error of the benchmarked field against the analytic solution at the last step
     del kev
@@ -311,9 +322,8 @@ def b200_arm(a):
 
     e2e = e2e_job(a, lay, local)
     if dist is not None:
-        t = torch.tensor([e2e["seconds"]], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e["value"] = round(world * e2e["points"] / t.item() / 1e9, 4)
+        (sec,) = max_over_ranks(dist, [e2e["seconds"]], "cuda")
+        e2e["value"] = round(job_gpoints(world, e2e["points"], 1, sec), 4)
 
     cpu = None
     if rank == 0 and not a.no_cpu:

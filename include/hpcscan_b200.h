@@ -96,7 +96,7 @@ int         b200_copy_box_h2d(const b200_layout* lay, int elem_size, void* dev, 
 		const b200_box* box, void* stream);
 
 /* ---- fills ---------------------------------------------------------------------------------
- * Grid::fill(pointType, val) (src/grid.cpp:1808-1826). */
+ * Grid::fill(pointType, val) (src/grid.cpp:1802-1824). */
 int b200_fill_const(const b200_layout* lay, b200_field u, const b200_box* box, double val,
 		void* stream);
 
@@ -157,20 +157,20 @@ int b200_propagate_step(const b200_layout* lay, int order, b200_field prn, b200_
 		b200_field coef, double inv2_1, double inv2_2, double inv2_3, int bc_type, void* stream);
 
 /* ---- norms (FP64 accumulation; synchronous on `stream`) ------------------------------------
- * Grid::getSumAbs (src/grid.cpp:2230-2273). */
+ * Grid::getSumAbs (src/grid.cpp:2229-2274). */
 int b200_sum_abs(const b200_layout* lay, b200_field u, const b200_box* box, double* out,
 		void* stream);
-/* Grid::getSumAbsDiff (src/grid.cpp:2176-2227): sum |u1 - u2|. */
+/* Grid::getSumAbsDiff (src/grid.cpp:2173-2225): sum |u1 - u2|. */
 int b200_sum_abs_diff(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
 		double* out, void* stream);
-/* Grid::L1Err (src/grid.cpp:2058-2110) in one pass: sum |u1 - u2| and sum |u2|. */
+/* Grid::L1Err (src/grid.cpp:2058-2109) in one pass: sum |u1 - u2| and sum |u2|. */
 int b200_l1_sums(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
 		double* sum_abs_diff, double* sum_abs_ref, void* stream);
-/* Grid::maxErr (src/grid.cpp:2006-2055): max over the box of |u1-u2|/|u2|, or |u1-u2|
+/* Grid::maxErr (src/grid.cpp:2006-2054): max over the box of |u1-u2|/|u2|, or |u1-u2|
  * where |(float)u2| < max_err_float (MAX_ERR_FLOAT, src/constant.h:14-20). */
 int b200_max_err(const b200_layout* lay, b200_field u1, b200_field u2, const b200_box* box,
 		double max_err_float, double* out, void* stream);
-/* Grid::getMin / getMax (src/grid.cpp:2276-2336), both in one pass. */
+/* Grid::getMin / getMax (src/grid.cpp:2278-2334), both in one pass. */
 int b200_min_max(const b200_layout* lay, b200_field u, const b200_box* box, double* mn,
 		double* mx, void* stream);
 
