@@ -40,6 +40,14 @@ class Field(ctypes.Structure):
     _fields_ = [("data", ctypes.c_void_p), ("dtype", ctypes.c_int32), ("scale", ctypes.c_float)]
 
 
+class Shot(ctypes.Structure):
+    _fields_ = [("lay", Layout), ("inv2", ctypes.c_double * 3), ("coef", ctypes.c_void_p),
+                ("sponge", ctypes.c_void_p * 3), ("src", ctypes.c_int64), ("amp", ctypes.c_float),
+                ("wavelet", ctypes.c_void_p), ("nrec", ctypes.c_int), ("rec", ctypes.c_void_p),
+                ("traces", ctypes.c_void_p), ("dobs", ctypes.c_void_p), ("wave", ctypes.c_void_p),
+                ("adj", ctypes.c_void_p), ("grad", ctypes.c_void_p)]
+
+
 def build(quiet: bool = True) -> None:
     """Compile every CUDA source of hpcscan_b200/csrc for sm_100a into libhpcscan_b200.so."""
     subprocess.run(["make", "-C", os.path.join(HERE, "csrc"), "-j8"], check=True,
@@ -85,6 +93,12 @@ SIGNATURES = {
     "b200_l1_sums_separable_noalloc": [_PL, Field, _PB, _VP, _VP, _VP, _D, _I, _PD, _PD, _VP],
     "b200_device_status": [ctypes.POINTER(_I), _I],
     "b200_stencil_route": [_PL, _I, _I, ctypes.POINTER(_I)],
+    "b200_batch_create": [ctypes.POINTER(_VP), _I, _I, _I, ctypes.POINTER(Shot), _D, _I],
+    "b200_batch_destroy": [_VP],
+    "b200_batch_forward_step": [_VP, _I, _I, _I, _I, _VP],
+    "b200_batch_adjoint_step": [_VP, _I, _I, _VP],
+    "b200_batch_gradient": [_VP, _I, _I, _VP],
+    "b200_batch_info": [_VP, ctypes.POINTER(_I)],
     "b200_set_arith_mode": [_I],
     "b200_get_arith_mode": [ctypes.POINTER(_I)],
     "b200_set_stencil_config": [_I, _I, _I, _I, _I],
@@ -92,6 +106,7 @@ SIGNATURES = {
     "b200_autotune_stencil": [_PL, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), _PD],
 }
 B200_ARITH_EXACT, B200_ARITH_FMA = 0, 1
+B200_BATCH_ADJOINT, B200_BATCH_GRADIENT = 1, 2
 B200_ARRAY_FILL, B200_ARRAY_COPY, B200_ARRAY_ADD, B200_ARRAY_MUL, B200_ARRAY_ADD_UPDATE = range(5)
 OP_FD_D2_N1, OP_FD_D2_N2, OP_FD_D2_N3, OP_LAPLACIAN, OP_PRESSURE, OP_STEP = 1, 2, 3, 4, 5, 6
 _RESTYPE = {"b200_last_error": ctypes.c_char_p}

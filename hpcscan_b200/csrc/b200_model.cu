@@ -1,0 +1,344 @@
+// Acoustic modelling engine: batches of shots (each with its own grid, model, source and
+// receivers) stepped forward and backward in lockstep, one launch per stencil pass for the whole
+// batch, for the adjoint-state gradient of the receiver data misfit with respect to the squared
+// slowness. The reference's propagator step (src/grid.cpp:4612-5113) with an absorbing sponge
+// and a point source; the reference has no adjoint and no batching.
+//
+// Per shot, FP32 (the damping G = g1(i1) g2(i2) g3(i3), C = (v dt)^2):
+//   forward   p[n+1] = G (2 p[n] + C Lap p[n]) - G^2 p[n-1] ; p[n+1](src) += G amp s[n]
+//             traces[n] = p[n+1](receivers)
+//   adjoint   w[k] = G (2 w[k+1] + C Lap w[k+1]) - G^2 w[k+2] ; w[k](rec) += C G (d[k] - dobs[k])
+//   gradient  g += -(C / dt^2) w[n+1] Lap p[n]
+// The stencil passes are k_zmarch_batch launches (b200_zmarch.cuh, MODE_MODEL / MODE_GRAD) over
+// slotted grids: every shot keeps its forward wavefields in `nslot` consecutive grids and its
+// adjoint wavefields in 2, and each call names the slots it reads and writes. No call allocates
+// or synchronises, so a whole schedule can be captured in a CUDA graph.
+#include <cstdlib>
+#include <vector>
+
+#include "b200_zmarch.cuh"
+
+namespace b200 {
+namespace {
+
+// Shot data the small per-step kernels need (device copy, one per shot).
+struct MShot {
+	float* wave;                  // nslot x field
+	float* adj;                   // 2 x field (or nullptr)
+	int64_t field;                // elements per grid
+	const float* coef;
+	const float* g1;
+	const float* g2;
+	const float* g3;
+	int64_t n1, n12;
+	int64_t src;
+	float amp;
+	const float* wavelet;
+	int nrec;
+	const int64_t* rec;
+	float* traces;
+	const float* dobs;
+};
+
+__device__ __forceinline__ float damping(const MShot& m, int64_t ii)
+{
+	const int64_t z = ii / m.n12, r = ii - z * m.n12, y = r / m.n1, x = r - y * m.n1;
+	return m.g1[x] * (m.g2[y] * m.g3[z]);
+}
+
+// Source injection into slot `slot` of every shot, then the receivers of that slot into row n.
+__global__ void k_model_source_record(const MShot* __restrict__ shots, int n, int slot)
+{
+	const MShot& m = shots[blockIdx.x];
+	float* p = m.wave + slot * m.field;
+	if (threadIdx.x == 0) {
+		const float g = damping(m, m.src);
+		p[m.src] = fmaf(g * m.amp, m.wavelet[n], p[m.src]);
+	}
+	__syncthreads();
+	for (int r = threadIdx.x; r < m.nrec; r += blockDim.x)
+		m.traces[(int64_t)n * m.nrec + r] = p[m.rec[r]];
+}
+
+// Residual injection d[k] - dobs[k] (row k - 1) into adjoint slot `slot` at the receivers.
+__global__ void k_model_residual(const MShot* __restrict__ shots, int k, int slot)
+{
+	const MShot& m = shots[blockIdx.x];
+	float* w = m.adj + slot * m.field;
+	const int64_t row = (int64_t)(k - 1) * m.nrec;
+	for (int r = threadIdx.x; r < m.nrec; r += blockDim.x) {
+		const int64_t ii = m.rec[r];
+		const float res = m.traces[row + r] - m.dobs[row + r];
+		w[ii] = fmaf(m.coef[ii] * damping(m, ii), res, w[ii]);
+	}
+}
+
+// Stencil passes: R and the tile shape (shape 0), FP32 with fused multiply-adds.
+template <int R, int MODE>
+using ModelCfg = ZCfg<float, R, MODE, Shape<float, R, 0>::TX, Shape<float, R, 0>::TY,
+		Shape<float, R, 0>::VY, Shape<float, R, 0>::PF, false, Shape<float, R, 0>::MINB>;
+
+}  // namespace
+}  // namespace b200
+
+using namespace b200;
+
+struct b200_batch {
+	int R = 0;
+	int nshot = 0;
+	int nslot = 0;
+	int ctas = 0;                   // CTAs of one stencil pass over the whole batch
+	int smem[3] = {0, 0, 0};
+	ZShot* d_fwd = nullptr;         // stencil tables: forward, adjoint, gradient
+	ZShot* d_adj = nullptr;
+	ZShot* d_grad = nullptr;
+	MShot* d_m = nullptr;
+	bool has_adj = false, has_grad = false;
+};
+
+namespace {
+
+template <int R>
+int batch_tables(b200_batch* b, const b200_shot* shots, double dt, std::vector<ZShot>& fwd,
+		std::vector<ZShot>& adj, std::vector<ZShot>& grad)
+{
+	using CF = ModelCfg<R, MODE_MODEL>;
+	using CG = ModelCfg<R, MODE_GRAD>;
+	static_assert(CF::TX == CG::TX && CF::TY == CG::TY && CF::BX == CG::BX && CF::BY == CG::BY,
+			"one tiling for every pass");
+	int cta = 0;
+	for (int i = 0; i < b->nshot; i++) {
+		const b200_shot& sh = shots[i];
+		const b200_layout* lay = &sh.lay;
+		ZShot z;
+		std::memset(&z, 0, sizeof(z));
+		ZArgs<float>& a = z.a;
+		a.n1 = lay->n1;
+		a.n12 = lay->n1 * lay->n2;
+		a.x_start = (int)(lay->s1 / CF::VX) * CF::VX;
+		a.s1 = (int)lay->s1; a.e1 = (int)lay->e1;
+		a.s2 = (int)lay->s2; a.e2 = (int)lay->e2;
+		a.s3 = (int)lay->s3; a.e3 = (int)lay->e3;
+		a.inv2_1 = (float)sh.inv2[0];
+		a.inv2_2 = (float)sh.inv2[1];
+		a.inv2_3 = (float)sh.inv2[2];
+		a.coef_scale = 1.0f;
+		a.timeout_ns = 2000000000ull;
+		if (int rc = device_error_word(&a.err)) return rc;
+		a.g1 = sh.sponge[0];
+		a.g2 = sh.sponge[1];
+		a.g3 = sh.sponge[2];
+		a.kscale = (float)(-1.0 / (dt * dt));
+		z.ntx = (a.e1 + 1 - a.x_start + CF::TX - 1) / CF::TX;
+		z.nty = (a.e2 - a.s2 + 1 + CF::TY - 1) / CF::TY;
+		const int nz = a.e3 - a.s3 + 1;
+		a.nz_chunk = nz < 64 ? nz : 64;
+		z.nzc = (nz + a.nz_chunk - 1) / a.nz_chunk;
+		z.cta_begin = cta;
+		cta += z.ntx * z.nty * z.nzc;
+		const int64_t field = lay->n1 * lay->n2 * lay->n3;
+		// forward: u = wave, p0 = wave (p[n-1]), p1 = coef, out = wave
+		ZShot f = z;
+		f.a.out = sh.wave;
+		f.a.out_slot_stride = field;
+		int rc = make_map_slots(&f.tm[0], sh.wave, lay, b->nslot, CF::BX, CF::BY);
+		if (!rc) rc = make_map_slots(&f.tm[1], sh.wave, lay, b->nslot, CF::TX, CF::TY);
+		if (!rc) rc = make_map_slots(&f.tm[2], sh.coef, lay, 1, CF::TX, CF::TY);
+		if (!rc) f.tm[3] = f.tm[2];
+		if (rc) return rc;
+		fwd.push_back(f);
+		if (b->has_adj) {
+			ZShot w = z;
+			w.a.out = sh.adj;
+			w.a.out_slot_stride = field;
+			rc = make_map_slots(&w.tm[0], sh.adj, lay, 2, CF::BX, CF::BY);
+			if (!rc) rc = make_map_slots(&w.tm[1], sh.adj, lay, 2, CF::TX, CF::TY);
+			if (!rc) w.tm[2] = f.tm[2];
+			if (!rc) w.tm[3] = f.tm[2];
+			if (rc) return rc;
+			adj.push_back(w);
+		}
+		if (b->has_grad) {
+			// gradient: u = wave (p[n]), p0 = adj (w[n+1]), p1 = coef, p2 = grad, out = grad
+			ZShot g = z;
+			g.a.out = sh.grad;
+			g.a.out_slot_stride = 0;
+			g.tm[0] = f.tm[0];
+			rc = make_map_slots(&g.tm[1], sh.adj, lay, 2, CF::TX, CF::TY);
+			if (!rc) g.tm[2] = f.tm[2];
+			if (!rc) rc = make_map_slots(&g.tm[3], sh.grad, lay, 1, CF::TX, CF::TY);
+			if (rc) return rc;
+			grad.push_back(g);
+		}
+	}
+	b->ctas = cta;
+	b->smem[0] = CF::SMEM;
+	b->smem[1] = CF::SMEM;
+	b->smem[2] = CG::SMEM;
+	int rc = cuda_error(cudaFuncSetAttribute(k_zmarch_batch<CF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			CF::SMEM), "cudaFuncSetAttribute(k_zmarch_batch)");
+	if (!rc)
+		rc = cuda_error(cudaFuncSetAttribute(k_zmarch_batch<CG>,
+				cudaFuncAttributeMaxDynamicSharedMemorySize, CG::SMEM),
+				"cudaFuncSetAttribute(k_zmarch_batch)");
+	return rc;
+}
+
+template <int R, int MODE>
+int launch_pass(const b200_batch* b, const ZShot* table, int su, int sp0, int sout, cudaStream_t s)
+{
+	using Cfg = ModelCfg<R, MODE>;
+	k_zmarch_batch<Cfg><<<b->ctas, Cfg::NT, Cfg::SMEM, s>>>(table, b->nshot, su, sp0, sout);
+	return check_launch("k_zmarch_batch");
+}
+
+int dispatch_pass(const b200_batch* b, int mode, const ZShot* table, int su, int sp0, int sout,
+		cudaStream_t s)
+{
+	return dispatch_order(2 * b->R, [&](auto rt) {
+		constexpr int R = decltype(rt)::value;
+		if (mode == MODE_GRAD) return launch_pass<R, MODE_GRAD>(b, table, su, sp0, sout, s);
+		return launch_pass<R, MODE_MODEL>(b, table, su, sp0, sout, s);
+	});
+}
+
+int check_shot(const b200_shot& sh, int order, bool need_adj, bool need_grad, int i)
+{
+	const b200_layout* lay = &sh.lay;
+	if (int rc = check_layout(lay)) return rc;
+	if (lay->dim != 3) return set_error(B200_ERR_UNSUPPORTED, "shot %d: the modelling engine is 3-D", i);
+	if (lay->halo != order / 2) return set_error(B200_ERR_ARG, "shot %d: halo %d for order %d", i, lay->halo, order);
+	if ((lay->n1 * 4) % 16) return set_error(B200_ERR_ARG, "shot %d: n1 * 4 bytes not a multiple of 16", i);
+	if (!sh.wave || !sh.coef || !sh.sponge[0] || !sh.sponge[1] || !sh.sponge[2] || !sh.wavelet)
+		return set_error(B200_ERR_ARG, "shot %d: NULL wave/coef/sponge/wavelet", i);
+	if ((reinterpret_cast<uintptr_t>(sh.wave) | reinterpret_cast<uintptr_t>(sh.coef)) % 16)
+		return set_error(B200_ERR_ARG, "shot %d: grids must be 16-byte aligned", i);
+	if (sh.nrec < 0 || (sh.nrec > 0 && (!sh.rec || !sh.traces)))
+		return set_error(B200_ERR_ARG, "shot %d: receivers", i);
+	const int64_t np = lay->n1 * lay->n2 * lay->n3;
+	if (sh.src < 0 || sh.src >= np) return set_error(B200_ERR_ARG, "shot %d: source index", i);
+	if (need_adj && (!sh.adj || !sh.dobs || reinterpret_cast<uintptr_t>(sh.adj) % 16))
+		return set_error(B200_ERR_ARG, "shot %d: adjoint needs adj (16-byte aligned) and dobs", i);
+	if (need_grad && (!sh.grad || reinterpret_cast<uintptr_t>(sh.grad) % 16))
+		return set_error(B200_ERR_ARG, "shot %d: gradient needs grad (16-byte aligned)", i);
+	return B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200_batch_create(b200_batch** out, int order, int nslot, int nshot, const b200_shot* shots,
+		double dt, int flags)
+{
+	if (!out) return set_error(B200_ERR_ARG, "batch is NULL");
+	*out = nullptr;
+	if (int rc = check_order(order)) return rc;
+	if (nshot < 1 || !shots) return set_error(B200_ERR_ARG, "no shots");
+	if (nslot < 2) return set_error(B200_ERR_ARG, "nslot %d < 2", nslot);
+	if (!(dt > 0.0)) return set_error(B200_ERR_ARG, "dt %g", dt);
+	const bool adj = flags & B200_BATCH_ADJOINT, grad = flags & B200_BATCH_GRADIENT;
+	for (int i = 0; i < nshot; i++)
+		if (int rc = check_shot(shots[i], order, adj || grad, grad, i)) return rc;
+	b200_batch* b = new b200_batch;
+	b->R = order / 2;
+	b->nshot = nshot;
+	b->nslot = nslot;
+	b->has_adj = adj || grad;
+	b->has_grad = grad;
+	std::vector<ZShot> fwd, ad, gr;
+	int rc = dispatch_order(order, [&](auto rt) {
+		constexpr int R = decltype(rt)::value;
+		return batch_tables<R>(b, shots, dt, fwd, ad, gr);
+	});
+	std::vector<MShot> ms(nshot);
+	for (int i = 0; i < nshot && !rc; i++) {
+		const b200_shot& sh = shots[i];
+		MShot& m = ms[i];
+		m.wave = sh.wave;
+		m.adj = sh.adj;
+		m.field = sh.lay.n1 * sh.lay.n2 * sh.lay.n3;
+		m.coef = sh.coef;
+		m.g1 = sh.sponge[0];
+		m.g2 = sh.sponge[1];
+		m.g3 = sh.sponge[2];
+		m.n1 = sh.lay.n1;
+		m.n12 = sh.lay.n1 * sh.lay.n2;
+		m.src = sh.src;
+		m.amp = sh.amp;
+		m.wavelet = sh.wavelet;
+		m.nrec = sh.nrec;
+		m.rec = sh.rec;
+		m.traces = sh.traces;
+		m.dobs = sh.dobs;
+	}
+	auto upload = [&](auto** dst, const auto& v) -> int {
+		if (v.empty()) return B200_OK;
+		const size_t bytes = sizeof(v[0]) * v.size();
+		int r = cuda_error(cudaMalloc(reinterpret_cast<void**>(dst), bytes), "cudaMalloc(batch)");
+		if (!r) r = cuda_error(cudaMemcpy(*dst, v.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(batch)");
+		return r;
+	};
+	if (!rc) rc = upload(&b->d_fwd, fwd);
+	if (!rc) rc = upload(&b->d_adj, ad);
+	if (!rc) rc = upload(&b->d_grad, gr);
+	if (!rc) rc = upload(&b->d_m, ms);
+	if (rc) {
+		b200_batch_destroy(b);
+		return rc;
+	}
+	*out = b;
+	return B200_OK;
+}
+
+int b200_batch_destroy(b200_batch* b)
+{
+	if (!b) return B200_OK;
+	cudaFree(b->d_fwd);
+	cudaFree(b->d_adj);
+	cudaFree(b->d_grad);
+	cudaFree(b->d_m);
+	delete b;
+	return B200_OK;
+}
+
+int b200_batch_forward_step(b200_batch* b, int n, int scur, int sprev, int sout, void* stream)
+{
+	if (!b) return set_error(B200_ERR_ARG, "batch is NULL");
+	if (scur < 0 || scur >= b->nslot || sprev < 0 || sprev >= b->nslot || sout < 0 ||
+			sout >= b->nslot || sout == scur)
+		return set_error(B200_ERR_ARG, "forward slots %d %d %d of %d", scur, sprev, sout, b->nslot);
+	if (n < 0) return set_error(B200_ERR_ARG, "step %d", n);
+	cudaStream_t s = as_stream(stream);
+	if (int rc = dispatch_pass(b, MODE_MODEL, b->d_fwd, scur, sprev, sout, s)) return rc;
+	k_model_source_record<<<b->nshot, 256, 0, s>>>(b->d_m, n, sout);
+	return check_launch("k_model_source_record");
+}
+
+int b200_batch_adjoint_step(b200_batch* b, int k, int scur, void* stream)
+{
+	if (!b || !b->has_adj) return set_error(B200_ERR_ARG, "batch without adjoint wavefields");
+	if (scur < 0 || scur > 1 || k < 1) return set_error(B200_ERR_ARG, "adjoint step %d slot %d", k, scur);
+	cudaStream_t s = as_stream(stream);
+	const int o = 1 - scur;
+	if (int rc = dispatch_pass(b, MODE_MODEL, b->d_adj, scur, o, o, s)) return rc;
+	k_model_residual<<<b->nshot, 256, 0, s>>>(b->d_m, k, o);
+	return check_launch("k_model_residual");
+}
+
+int b200_batch_gradient(b200_batch* b, int swave, int sadj, void* stream)
+{
+	if (!b || !b->has_grad) return set_error(B200_ERR_ARG, "batch without gradient");
+	if (swave < 0 || swave >= b->nslot || sadj < 0 || sadj > 1)
+		return set_error(B200_ERR_ARG, "gradient slots %d %d", swave, sadj);
+	return dispatch_pass(b, MODE_GRAD, b->d_grad, swave, sadj, 0, as_stream(stream));
+}
+
+int b200_batch_info(const b200_batch* b, int* ctas_per_pass)
+{
+	if (!b || !ctas_per_pass) return set_error(B200_ERR_ARG, "NULL");
+	*ctas_per_pass = b->ctas;
+	return B200_OK;
+}
+
+}  // extern "C"

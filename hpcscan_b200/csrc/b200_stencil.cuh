@@ -12,6 +12,8 @@ enum StencilMode {
 	MODE_LAPLACIAN = 4,  // Grid::FD_LAPLACIAN
 	MODE_PRESSURE = 5,   // Grid::computePressureWithFD (in = prc, out = prn)
 	MODE_STEP = 6,       // applyBoundaryCondition(prc) fused with computePressureWithFD
+	MODE_MODEL = 7,      // damped leapfrog of the modelling engine: p+ = G (2 p + C Lap p) - G^2 p-
+	MODE_GRAD = 8,       // gradient accumulation: g += k C w Lap p
 };
 
 // Validating front end shared by all stencil entry points.

@@ -120,6 +120,27 @@ int make_map(CUtensorMap* m, const void* base, int dtype, const b200_layout* lay
 	return B200_OK;
 }
 
+int make_map_slots(CUtensorMap* m, const void* base, const b200_layout* lay, int nslot, int bx,
+		int by)
+{
+	EncodeTiledFn enc;
+	if (int rc = get_encode(&enc)) return rc;
+	const cuuint64_t es = 4;
+	const cuuint64_t dims[4] = {(cuuint64_t)lay->n1, (cuuint64_t)lay->n2, (cuuint64_t)lay->n3,
+	                            (cuuint64_t)nslot};
+	const cuuint64_t strides[3] = {lay->n1 * es, lay->n1 * lay->n2 * es,
+	                               lay->n1 * lay->n2 * lay->n3 * es};
+	const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, 1};
+	const cuuint32_t estr[4] = {1, 1, 1, 1};
+	std::memset(m, 0, sizeof(*m));
+	CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), dims, strides,
+			box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+			CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS)
+		return set_error(B200_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for a slotted grid", (int)r);
+	return B200_OK;
+}
+
 bool zmarch_accepts(const b200_layout* lay, int dtype)
 {
 	if (lay->dim != 3) return false;

@@ -114,6 +114,25 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, in
 			: "memory");
 }
 
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int x, int y, int z,
+		int w, uint64_t* bar)
+{
+	asm volatile(
+			"cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+			" [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+			"l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+			: "memory");
+}
+
+// A tile load of a 3-D grid, or of slot `w` of a slotted (4-D) grid.
+template <bool SLOTS>
+__device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* tm, int x, int y, int z,
+		int w, uint64_t* bar)
+{
+	if constexpr (SLOTS) tma_load_4d(dst, tm, x, y, z, w, bar);
+	else tma_load_3d(dst, tm, x, y, z, bar);
+}
+
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* tm)
 {
 	asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");
@@ -151,14 +170,17 @@ struct ZCfg {
 	static constexpr bool XH = (MODE == MODE_D2_AXIS1 || MODE >= MODE_LAPLACIAN);
 	static constexpr bool YH = (MODE == MODE_D2_AXIS2 || MODE >= MODE_LAPLACIAN);
 	static constexpr bool ZQ = (MODE == MODE_D2_AXIS3 || MODE >= MODE_LAPLACIAN);
-	static constexpr bool P = (MODE == MODE_PRESSURE || MODE == MODE_STEP);
+	static constexpr bool P = (MODE == MODE_PRESSURE || MODE == MODE_STEP || MODE == MODE_MODEL ||
+	                           MODE == MODE_GRAD);
+	// pointwise tiles of the output plane: prn + coef (pressure, model), w + C + g (gradient)
+	static constexpr int NPT = (MODE == MODE_GRAD) ? 3 : 2;
 	static constexpr int R4 = XH ? round_up(R, VX) : 0;     // x halo, whole vectors
 	static constexpr int RY = YH ? R : 0;
 	static constexpr int RZ = ZQ ? R : 0;
 	static constexpr int BX = TX + 2 * R4;
 	static constexpr int BY = TY + 2 * RY;
 	static constexpr int NSU = RZ + 1 + PF;                  // input-tile ring
-	static constexpr int NSP = P ? 1 + PF : 1;               // prn/coef ring
+	static constexpr int NSP = P ? 1 + PF : 1;               // pointwise-tile ring
 	static constexpr int U_BYTES = BX * BY * (int)sizeof(S);
 	static constexpr int U_STRIDE = round_up(U_BYTES, 128);
 	static constexpr int PT_BYTES = TX * TY * (int)sizeof(S);
@@ -167,13 +189,15 @@ struct ZCfg {
 	static constexpr int NC = NTX * (TY / VY);              // consumer threads
 	static constexpr int NWC = NC / 32;                      // consumer warps
 	static constexpr int NT = NC + 32;                       // + one producer warp
-	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * 2 * PT_STRIDE : 0) +
+	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * NPT * PT_STRIDE : 0) +
 	                            (2 * NSU + 2 * NSP) * 8;
 	// CTAs per SM the launch bounds ask for (registers follow: an SM has four sub-partitions
 	// of 16K registers and spreads a CTA's warps over them). Two CTAs per SM for R <= 4 with
 	// 8-warp CTAs; wider stencils keep their longer z queue in registers at one CTA per SM.
 	static constexpr int MINB = MINB_ > 0 ? MINB_ : ((NT <= 256 && R <= 4) ? 2 : 1);
 	static_assert(TX % VX == 0 && TY % VY == 0 && NC % 32 == 0, "tile shape");
+	static_assert((MODE != MODE_MODEL && MODE != MODE_GRAD) || std::is_same_v<S, float>,
+			"the modelling engine computes in FP32");
 	static_assert(BX <= 256 && BY <= 256, "TMA box limit");
 	static_assert((BX * sizeof(S)) % 16 == 0 && (TX * sizeof(S)) % 16 == 0, "TMA inner extent");
 };
@@ -189,6 +213,12 @@ struct ZArgs {
 	float coef_scale;
 	uint64_t timeout_ns;
 	unsigned int* err;         // device error word (b200_device_status)
+	// modelling engine (MODE_MODEL, MODE_GRAD): damping tables G = g1 g2 g3, gradient factor
+	const float* g1;
+	const float* g2;
+	const float* g3;
+	float kscale;
+	int64_t out_slot_stride;   // elements between slots of the output grid
 };
 
 
@@ -207,11 +237,13 @@ struct Ring {
 	}
 };
 
-template <class Cfg>
-__global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
-		const __grid_constant__ CUtensorMap tm_u,
-		const __grid_constant__ CUtensorMap tm_prn, const __grid_constant__ CUtensorMap tm_coef,
-		const ZArgs<typename Cfg::C> a)
+// The kernel body: one CTA, tile (bx, by) of (i1, i2), z-chunk bz. tm_p[0..NPT) are the
+// pointwise tiles of the output plane. SLOTS: the grids are slotted (4-D tensor maps whose
+// outermost coordinate is the slot), as the modelling engine keeps its wavefields.
+template <class Cfg, bool SLOTS>
+__device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUtensorMap* tm_p0,
+		const CUtensorMap* tm_p1, const CUtensorMap* tm_p2, const ZArgs<typename Cfg::C>& a,
+		int bx, int by, int bz, int slot_u, int slot_p0, int slot_out)
 {
 	using S = typename Cfg::Stor;
 	using C = typename Cfg::C;
@@ -229,16 +261,17 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 			(reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
 	S* su = reinterpret_cast<S*>(smem);
 	S* sp = reinterpret_cast<S*>(smem + NSU * Cfg::U_STRIDE);
+	constexpr int NPT = Cfg::NPT;
 	uint64_t* bars = reinterpret_cast<uint64_t*>(
-			smem + NSU * Cfg::U_STRIDE + (Cfg::P ? NSP * 2 * Cfg::PT_STRIDE : 0));
+			smem + NSU * Cfg::U_STRIDE + (Cfg::P ? NSP * NPT * Cfg::PT_STRIDE : 0));
 	uint64_t* full_u = bars;
 	uint64_t* empty_u = bars + NSU;
 	uint64_t* full_p = bars + 2 * NSU;
 	uint64_t* empty_p = full_p + NSP;
 
-	const int tile_x0 = a.x_start + (int)blockIdx.x * TX;
-	const int tile_y0 = a.s2 + (int)blockIdx.y * Cfg::TY;
-	const int z0 = a.s3 + (int)blockIdx.z * a.nz_chunk;
+	const int tile_x0 = a.x_start + bx * TX;
+	const int tile_y0 = a.s2 + by * Cfg::TY;
+	const int z0 = a.s3 + bz * a.nz_chunk;
 	const int z1 = min(z0 + a.nz_chunk, a.e3 + 1);
 	const int J = (z1 - z0) + 2 * RZ;          // planes this CTA streams in
 
@@ -259,10 +292,11 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 	if (threadIdx.x >= NC) {
 		// ---- producer: one thread issues every TMA copy ------------------------------------------
 		if (threadIdx.x != NC) return;
-		prefetch_tmap(&tm_u);
+		prefetch_tmap(tm_u);
 		if constexpr (Cfg::P) {
-			prefetch_tmap(&tm_prn);
-			prefetch_tmap(&tm_coef);
+			prefetch_tmap(tm_p0);
+			prefetch_tmap(tm_p1);
+			if constexpr (NPT > 2) prefetch_tmap(tm_p2);
 		}
 		int issued_u = 0, issued_p = 0;
 		bool ok = true;
@@ -281,7 +315,8 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 				else if (plane > a.e3) plane = 2 * a.e3 - plane;
 			}
 			mbar_arrive_expect_tx(&full_u[wu.slot], Cfg::U_BYTES);
-			tma_load_3d(su + wu.slot * UE, &tm_u, tile_x0 - R4, tile_y0 - RY, plane, &full_u[wu.slot]);
+			tma_tile<SLOTS>(su + wu.slot * UE, tm_u, tile_x0 - R4, tile_y0 - RY, plane, slot_u,
+					&full_u[wu.slot]);
 			issued_u = j + 1;
 			wu.advance();
 			if constexpr (Cfg::P) {
@@ -291,11 +326,14 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 						ok = false;
 						break;
 					}
-					mbar_arrive_expect_tx(&full_p[wp.slot], 2 * Cfg::PT_BYTES);
-					tma_load_3d(sp + (2 * wp.slot) * PE, &tm_prn, tile_x0, tile_y0, z0 + o,
+					mbar_arrive_expect_tx(&full_p[wp.slot], NPT * Cfg::PT_BYTES);
+					tma_tile<SLOTS>(sp + (NPT * wp.slot) * PE, tm_p0, tile_x0, tile_y0, z0 + o,
+							slot_p0, &full_p[wp.slot]);
+					tma_tile<SLOTS>(sp + (NPT * wp.slot + 1) * PE, tm_p1, tile_x0, tile_y0, z0 + o, 0,
 							&full_p[wp.slot]);
-					tma_load_3d(sp + (2 * wp.slot + 1) * PE, &tm_coef, tile_x0, tile_y0, z0 + o,
-							&full_p[wp.slot]);
+					if constexpr (NPT > 2)
+						tma_tile<SLOTS>(sp + (NPT * wp.slot + 2) * PE, tm_p2, tile_x0, tile_y0,
+								z0 + o, 0, &full_p[wp.slot]);
 					issued_p = o + 1;
 					wp.advance();
 				}
@@ -443,7 +481,7 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 			if constexpr (Cfg::P) {
 				if (alive && !__all_sync(FULL, mbar_wait(&full_p[rp.slot], rp.phase, deadline)))
 					alive = false;
-				pt = sp + (2 * rp.slot) * PE;
+				pt = sp + (NPT * rp.slot) * PE;
 			}
 			const bool kb = Cfg::BC && (k == a.s3 || k == a.e3);
 			if constexpr (Cfg::BC) {
@@ -536,6 +574,31 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 								r2 = dz;
 							} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
 								r2 = A2::add(A2::add(dx, dy), dz);
+							} else if constexpr (Cfg::MODE == MODE_MODEL) {
+								// p+ = G (2 p + C Lap p) - G^2 p-, G = g1 g2 g3 (points past the
+								// inner box are never stored: clamp their table reads)
+								const float gyz = a.g2[min(Y0 + v, a.e2)] * a.g3[k];
+								const float2 G = make_float2(a.g1[min(X + e, a.e1)] * gyz,
+										a.g1[min(X + e + 1, a.e1)] * gyz);
+								const int o = (yl + v) * TX + xl + e;
+								const float2 pm = make_float2(Storage<S>::load(pt[o]), Storage<S>::load(pt[o + 1]));
+								const float2 cf = make_float2(Storage<S>::load(pt[PE + o]),
+										Storage<S>::load(pt[PE + o + 1]));
+								const float2 pc = make_float2(yv[v + RY][e], yv[v + RY][e + 1]);
+								const float2 lap = A2::add(A2::add(dx, dy), dz);
+								const float2 t = A2::mac(A2::add(pc, pc), cf, lap);
+								const float2 gg = A2::mul(G, G);
+								r2 = A2::mac(A2::mul(make_float2(-gg.x, -gg.y), pm), G, t);
+							} else if constexpr (Cfg::MODE == MODE_GRAD) {
+								// g += k C w Lap p
+								const int o = (yl + v) * TX + xl + e;
+								const float2 w = make_float2(Storage<S>::load(pt[o]), Storage<S>::load(pt[o + 1]));
+								const float2 cf = make_float2(Storage<S>::load(pt[PE + o]),
+										Storage<S>::load(pt[PE + o + 1]));
+								const float2 g0 = make_float2(Storage<S>::load(pt[2 * PE + o]),
+										Storage<S>::load(pt[2 * PE + o + 1]));
+								const float2 kw = A2::mul(A2::mul(make_float2(a.kscale, a.kscale), cf), w);
+								r2 = A2::mac(g0, kw, A2::add(A2::add(dx, dy), dz));
 							} else {
 								float pn[2], cf[2];
 								pn[0] = Storage<S>::load(pt[(yl + v) * TX + xl + e]);
@@ -598,6 +661,7 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 					const int Y = Y0 + v;
 					if (Y <= a.e2) {
 						S* dst = static_cast<S*>(a.out) + X + (int64_t)Y * a.n1 + (int64_t)k * a.n12;
+						if constexpr (SLOTS) dst += slot_out * a.out_slot_stride;
 						if (X >= a.s1 && X + VX - 1 <= a.e1) {
 							uint4 pk;
 							S* ps = reinterpret_cast<S*>(&pk);
@@ -631,11 +695,47 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 	if (!alive && lane == 0) atomicOr(a.err, 2u);
 }
 
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
+		const __grid_constant__ CUtensorMap tm_u,
+		const __grid_constant__ CUtensorMap tm_prn, const __grid_constant__ CUtensorMap tm_coef,
+		const ZArgs<typename Cfg::C> a)
+{
+	zmarch_body<Cfg, false>(&tm_u, &tm_prn, &tm_coef, &tm_coef, a, (int)blockIdx.x,
+			(int)blockIdx.y, (int)blockIdx.z, 0, 0, 0);
+}
+
+// One shot of a batched launch: its tensor maps (slotted grids: u, pointwise tiles 0..2), its
+// arguments and its range of CTAs. Lives in device memory, 64-byte aligned.
+struct alignas(64) ZShot {
+	CUtensorMap tm[4];
+	ZArgs<float> a;
+	int cta_begin, ntx, nty, nzc;
+};
+
+// Every shot of a batch in one launch: CTA b works on the shot whose range holds b.
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch_batch(const ZShot* __restrict__ shots,
+		int nshot, int slot_u, int slot_p0, int slot_out)
+{
+	const int b = (int)blockIdx.x;
+	int s = 0;
+	while (s + 1 < nshot && shots[s + 1].cta_begin <= b) ++s;
+	const ZShot& sh = shots[s];
+	const int local = b - sh.cta_begin;
+	const int bx = local % sh.ntx, by = (local / sh.ntx) % sh.nty, bz = local / (sh.ntx * sh.nty);
+	zmarch_body<Cfg, true>(&sh.tm[0], &sh.tm[1], &sh.tm[2], &sh.tm[3], sh.a, bx, by, bz, slot_u,
+			slot_p0, slot_out);
+}
+
 }  // namespace
 
 // ---- host side ------------------------------------------------------------------------------------
 // Tensor map of a 3-D grid with box (bx, by, 1) (b200_stencil_zmarch.cu).
 int make_map(CUtensorMap* m, const void* base, int dtype, const b200_layout* lay, int bx, int by);
+// Tensor map of nslot consecutive FP32 grids of one layout (4-D, the slot outermost).
+int make_map_slots(CUtensorMap* m, const void* base, const b200_layout* lay, int nslot, int bx,
+		int by);
 
 namespace {
 
@@ -676,7 +776,7 @@ int launch_zmarch(const ZLaunch& L)
 		tm_p = tm_u;
 		tm_c = tm_u;
 	}
-	ZArgs<C> a;
+	ZArgs<C> a{};
 	a.out = out.data;
 	a.n1 = lay->n1;
 	a.n12 = lay->n1 * lay->n2;

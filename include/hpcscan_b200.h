@@ -199,6 +199,58 @@ int b200_l1_sums_separable_noalloc(const b200_layout* lay, b200_field u, const b
 		const double* v1, const double* v2, const double* v3, double amp, int ref_dtype,
 		double* sum_abs_diff, double* sum_abs_ref, void* stream);
 
+/* ---- acoustic modelling and adjoint gradient (no counterpart in the reference) ---------------
+ * A batch of shots, each on its own 3-D FP32 grid (its own size, model, source and receivers),
+ * stepped in lockstep: one launch per stencil pass for the whole batch. Per shot, with the
+ * damping G = g1(i1) g2(i2) g3(i3) of an absorbing sponge and C = (v dt)^2 (the reference's
+ * coef, src/propagator_Ac2.cpp:234), on the INNER points, halos held at zero:
+ *   forward   p[n+1] = G (2 p[n] + C Lap p[n]) - G^2 p[n-1];  p[n+1](src) += G amp wavelet[n];
+ *             traces[n][r] = p[n+1](rec[r])                     (n = 0..nt-1)
+ *   adjoint   w[k] = G (2 w[k+1] + C Lap w[k+1]) - G^2 w[k+2];
+ *             w[k](rec[r]) += C G (traces[k-1][r] - dobs[k-1][r])   (k = nt..1)
+ *   gradient  grad += -(C / dt^2) w[n+1] Lap p[n]: with J = 1/2 sum (traces - dobs)^2 and the
+ *             squared slowness m = 1/v^2, dJ/dm summed over the steps.
+ * The recursion of w is the exact transpose of the forward one (the Laplacian with zero halos is
+ * symmetric), so the gradient is that of the discrete misfit.
+ * Each shot keeps `nslot` forward grids (`wave`, consecutive, n1*n2*n3 each) and two adjoint
+ * grids (`adj`); every call names the slots it reads and writes, so a caller can keep a ring of
+ * recomputed forward wavefields for checkpointing. Calls enqueue kernels on `stream` and neither
+ * allocate nor synchronise (b200_batch_create allocates the batch's small device tables). The
+ * receivers of a shot must be distinct points. */
+typedef struct b200_shot {
+	b200_layout lay;            /* 3-D, FP32, halo = order/2, n1 * 4 bytes a multiple of 16   */
+	double inv2[3];             /* (1/d_a)^2                                                  */
+	const float* coef;          /* C = (v dt)^2 (device)                                      */
+	const float* sponge[3];     /* damping tables over n1, n2, n3 (device)                    */
+	int64_t src;                /* flat index of the source point                             */
+	float amp;                  /* source amplitude factor                                    */
+	const float* wavelet;       /* nt source samples (device)                                 */
+	int nrec;
+	const int64_t* rec;         /* nrec distinct flat receiver indices (device)               */
+	float* traces;              /* nt x nrec synthetic data, written by the forward steps     */
+	const float* dobs;          /* nt x nrec observed data (adjoint)                          */
+	float* wave;                /* nslot forward grids (device, 16-byte aligned)              */
+	float* adj;                 /* 2 adjoint grids (device), or NULL                          */
+	float* grad;                /* gradient of this shot (device), or NULL                    */
+} b200_shot;
+typedef struct b200_batch b200_batch;
+#define B200_BATCH_ADJOINT  1
+#define B200_BATCH_GRADIENT 2
+/* Build the batch (checks every shot, encodes its tensor maps, uploads the tables). dt is the
+ * common time step (the gradient factor -1/dt^2). */
+int b200_batch_create(b200_batch** batch, int order, int nslot, int nshot, const b200_shot* shots,
+		double dt, int flags);
+int b200_batch_destroy(b200_batch* batch);
+/* Forward step n of every shot: wave[sout] = G (2 wave[scur] + C Lap wave[scur]) - G^2 wave[sprev]
+ * (sout may equal sprev, not scur), then the source and the receivers of row n. */
+int b200_batch_forward_step(b200_batch* batch, int n, int scur, int sprev, int sout, void* stream);
+/* Adjoint step k of every shot: adj[1-scur] = w[k] from adj[scur] = w[k+1], adj[1-scur] = w[k+2]. */
+int b200_batch_adjoint_step(b200_batch* batch, int k, int scur, void* stream);
+/* grad += -(C/dt^2) adj[sadj] Lap wave[swave] for every shot. */
+int b200_batch_gradient(b200_batch* batch, int swave, int sadj, void* stream);
+/* CTAs of one stencil pass over the whole batch. */
+int b200_batch_info(const b200_batch* batch, int* ctas_per_pass);
+
 /* ---- arithmetic mode and tuning ---------------------------------------------------------------
  * B200_ARITH_EXACT (default): every multiply and add of the stencil operators is a separately
  * rounded IEEE operation in the reference's evaluation order, so FP32/FP64 results are

@@ -76,7 +76,73 @@ def lib():
             getattr(_lib, f"oracle_min_max_{suf}").argtypes = [P(_Layout), vp, P(_Box),
                                                                P(ctypes.c_double),
                                                                P(ctypes.c_double)]
+        d, vp, i64 = ctypes.c_double, ctypes.c_void_p, ctypes.c_int64
+        _lib.oracle_model_forward_f64.argtypes = [P(_Layout), ctypes.c_int, vp, vp, i64, d, vp,
+                                                  ctypes.c_int, ctypes.c_int, vp, d, d, d, vp, vp]
+        _lib.oracle_model_adjoint_f64.argtypes = [P(_Layout), ctypes.c_int, vp, vp, ctypes.c_int,
+                                                  ctypes.c_int, vp, d, d, d, vp, i64, vp, vp, d, vp]
+        _lib.oracle_model_gradient_f64.argtypes = [P(_Layout), ctypes.c_int, vp, vp, i64, d, vp,
+                                                   ctypes.c_int, ctypes.c_int, vp, d, d, d, vp, d,
+                                                   vp, P(ctypes.c_double)]
     return _lib
+
+
+# ---- FP64 modelling / adjoint (oracle_model.c) ----------------------------------------------------
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(ctypes.c_void_p)
+
+
+def model_forward(lay, C, G, src, amp, wavelet, rec, inv2, snapshots=False):
+    """Traces (nt x nrec) of the damped leapfrog with a point source; with snapshots also
+    p[0..nt] as an (nt + 1, npoint) array."""
+    C, pc = _d(C)
+    G, pg = _d(G)
+    w, pw = _d(wavelet)
+    rec = np.ascontiguousarray(rec, dtype=np.int64)
+    nt, nrec = len(wavelet), len(rec)
+    tr = np.zeros((nt, nrec))
+    snap = np.zeros((nt + 1, lay.npoint)) if snapshots else None
+    rc = lib().oracle_model_forward_f64(_L(lay), lay.order, pc, pg, int(src), float(amp), pw, nt,
+                                        nrec, rec.ctypes.data_as(ctypes.c_void_p), *inv2,
+                                        tr.ctypes.data_as(ctypes.c_void_p),
+                                        None if snap is None else snap.ctypes.data_as(ctypes.c_void_p))
+    assert rc == 0
+    return (tr, snap) if snapshots else tr
+
+
+def model_adjoint(lay, C, G, res, rec, src, inv2):
+    """The adjoint wavefield w[n+1] at the source point, n = 0..nt-1, driven by res."""
+    C, pc = _d(C)
+    G, pg = _d(G)
+    res, pr = _d(res)
+    rec = np.ascontiguousarray(rec, dtype=np.int64)
+    nt, nrec = res.shape
+    w_src = np.zeros(nt)
+    rc = lib().oracle_model_adjoint_f64(_L(lay), lay.order, pc, pg, nt, nrec,
+                                        rec.ctypes.data_as(ctypes.c_void_p), *inv2, pr, int(src),
+                                        w_src.ctypes.data_as(ctypes.c_void_p), None, 1.0, None)
+    assert rc == 0
+    return w_src
+
+
+def model_gradient(lay, C, G, src, amp, wavelet, rec, inv2, dobs, dt):
+    """(misfit, dJ/dm) for the squared slowness m (C = dt^2 / m)."""
+    C, pc = _d(C)
+    G, pg = _d(G)
+    w, pw = _d(wavelet)
+    dobs, po = _d(dobs)
+    rec = np.ascontiguousarray(rec, dtype=np.int64)
+    grad = np.zeros(lay.npoint)
+    J = ctypes.c_double()
+    rc = lib().oracle_model_gradient_f64(_L(lay), lay.order, pc, pg, int(src), float(amp), pw,
+                                         len(wavelet), len(rec),
+                                         rec.ctypes.data_as(ctypes.c_void_p), *inv2, po,
+                                         float(dt) ** 2, grad.ctypes.data_as(ctypes.c_void_p),
+                                         ctypes.byref(J))
+    assert rc == 0
+    return J.value, grad
 
 
 def _suf(lay):

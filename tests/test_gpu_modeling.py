@@ -1,0 +1,135 @@
+"""GPU modelling engine (b200_batch_*): forward traces and adjoint gradients of batched shots
+against the FP64 oracle (oracle/oracle_model.c), checkpoint and batch invariance, CUDA graphs."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ORDER, DX, NT, F0 = 8, 10.0, 150, 30.0
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hpcscan_b200.grid import init_device
+    init_device(0)
+    return torch
+
+
+def make_shots(torch, sizes=((36, 30, 40), (28, 36, 24)), seed=0, scale=1.0, dobs=None):
+    from hpcscan_b200.modeling import Shot, grf_velocity
+    shots = []
+    for i, n in enumerate(sizes):
+        vel = grf_velocity((n[2], n[1], n[0]), sigma=3.0, seed=seed + i, vmin=1600.0, vmax=2600.0)
+        if scale != 1.0:
+            z, y, x = torch.meshgrid(*[torch.arange(k, device=vel.device, dtype=torch.float32)
+                                       for k in (n[2], n[1], n[0])], indexing="ij")
+            blob = torch.exp(-((x - n[0] / 3) ** 2 + (y - n[1] / 2) ** 2 + (z - n[2] / 2) ** 2) / 50.0)
+            vel = vel / torch.sqrt(1.0 + (scale - 1.0) * blob)      # m = 1/v^2 times (1 + a blob)
+        rec = np.array([(2, j, k) for j in range(2, n[1] - 2, 4) for k in range(2, n[2] - 2, 4)])
+        shots.append(Shot(n=n, dx=DX, vel=vel, src=(3, n[1] // 2, n[2] // 2), rec=rec, amp=2.0,
+                          sponge=6, dobs=None if dobs is None else dobs[i]))
+    return shots
+
+
+def dt_of():
+    from hpcscan_b200.modeling import stable_dt
+    return stable_dt(ORDER, DX, 2700.0)
+
+
+def oracle_inputs(batch, i):
+    """FP64 copies of exactly what shot i of the batch computes with."""
+    st = batch.states[i]
+    lay = st.lay
+    C = st.coef.double().cpu().numpy()
+    g = [t.cpu().numpy() for t in st.sponge]
+    G = (g[0][None, None, :] * (g[1][None, :, None] * g[2][:, None, None])).astype(np.float32)
+    G = G.reshape(-1).astype(np.float64)
+    inv2 = tuple(float(np.float32(1.0 / DX) * np.float32(1.0 / DX)) for _ in range(3))
+    return lay, C, G, st.src_flat, st.rec.cpu().numpy(), inv2, st.wavelet.double().cpu().numpy()
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def test_forward_traces_match_fp64_oracle(gpu):
+    from hpcscan_b200.modeling import Batch
+    from oracle import oracle
+    b = Batch(make_shots(gpu), ORDER, dt_of(), NT, F0)
+    b.forward()
+    gpu.cuda.synchronize()
+    for i in range(2):
+        lay, C, G, src, rec, inv2, wav = oracle_inputs(b, i)
+        want = oracle.model_forward(lay, C, G, src, 2.0, wav, rec, inv2)
+        got = b.traces(i).double().cpu().numpy()
+        assert np.abs(want).max() > 0
+        assert rel(got, want) < 2e-5, rel(got, want)
+    b.close()
+
+
+def observed(gpu, sizes=((36, 30, 40), (28, 36, 24))):
+    from hpcscan_b200.modeling import Batch
+    b = Batch(make_shots(gpu, sizes, scale=1.25), ORDER, dt_of(), NT, F0)
+    b.forward()
+    gpu.cuda.synchronize()
+    d = [b.traces(i).clone() for i in range(len(sizes))]
+    b.close()
+    return d
+
+
+def test_gradient_matches_fp64_oracle_and_is_checkpoint_invariant(gpu):
+    from hpcscan_b200.modeling import Batch
+    from oracle import oracle
+    dobs = observed(gpu)
+    grads = {}
+    for k in (7, NT):
+        b = Batch(make_shots(gpu, dobs=dobs), ORDER, dt_of(), NT, F0, gradient=True, checkpoint=k)
+        b.forward()
+        b.backward()
+        gpu.cuda.synchronize()
+        grads[k] = [b.states[i].grad.clone() for i in range(2)]
+        if k == 7:
+            for i in range(2):
+                lay, C, G, src, rec, inv2, wav = oracle_inputs(b, i)
+                J, g = oracle.model_gradient(lay, C, G, src, 2.0, wav, rec, inv2,
+                                             dobs[i].double().cpu().numpy(), b.dt)
+                got = b.states[i].grad.double().cpu().numpy()
+                assert np.abs(g).max() > 0
+                assert rel(got, g) < 1e-3, rel(got, g)
+                assert b.misfit(i) == pytest.approx(J, rel=1e-4)
+        b.close()
+    for i in range(2):
+        assert gpu.equal(grads[7][i], grads[NT][i])
+
+
+def test_batch_equals_single_shots_and_graph_equals_eager(gpu):
+    from hpcscan_b200.modeling import Batch, run_graph
+    dobs = observed(gpu)
+    b = Batch(make_shots(gpu, dobs=dobs), ORDER, dt_of(), NT, F0, gradient=True, checkpoint=11)
+    b.forward()
+    b.backward()
+    gpu.cuda.synchronize()
+    both = [(b.traces(i).clone(), b.states[i].grad.clone()) for i in range(2)]
+    # the same schedule captured in one CUDA graph and replayed
+    g = run_graph(lambda s: (b.forward(s), b.backward(s)))
+    for st in b.states:
+        st.grad.zero_()
+        st.traces.zero_()
+    g.replay()
+    gpu.cuda.synchronize()
+    for i in range(2):
+        assert gpu.equal(b.traces(i), both[i][0]) and gpu.equal(b.states[i].grad, both[i][1])
+    del g
+    b.close()
+    for i, n in enumerate(((36, 30, 40), (28, 36, 24))):
+        one = Batch(make_shots(gpu, (n,), seed=i, dobs=[dobs[i]]), ORDER, dt_of(), NT, F0,
+                    gradient=True, checkpoint=11)
+        one.forward()
+        one.backward()
+        gpu.cuda.synchronize()
+        assert gpu.equal(one.traces(0), both[i][0])
+        assert gpu.equal(one.states[0].grad, both[i][1])
+        one.close()
