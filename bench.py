@@ -58,6 +58,12 @@ def parse_args():
     p.add_argument("--cpu-steps", type=int, default=200,
                    help="time steps of the bounded reference CPU sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--workload", default="propa", choices=["propa", "adjoint", "modeling"],
+                   help="propa (default, the headline), adjoint (batched checkpointed gradients) "
+                        "or modeling (batched uneven forward shots)")
+    p.add_argument("--shots", type=int, default=0, help="shots (adjoint: 16, modeling: 64)")
+    p.add_argument("--nt", type=int, default=0, help="time steps (adjoint: 2000, modeling: 1500)")
+    p.add_argument("--checkpoint", type=int, default=45, help="adjoint checkpoint interval")
     return p.parse_args()
 
 
@@ -431,8 +437,226 @@ def e2e_job(a, lay, device):
                     "the periodic analytic-check norms)"}
 
 
+# ---- batched modelling and adjoint workloads ------------------------------------------------------
+
+def _surface_shots(n, nshot, seed):
+    """Distinct seeded source positions on the surface plane i1 = 1, off the receiver lattice."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out, seen = [], set()
+    while len(out) < nshot:
+        j, k = (int(v) for v in rng.integers(n // 8, n - n // 8, size=2))
+        if j % 4 == 0 and k % 4 == 0:
+            j += 1
+        if (j, k) not in seen:
+            seen.add((j, k))
+            out.append((1, j, k))
+    return out
+
+
+def _timed(fn, reps=1):
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def adjoint_arm(a):
+    """Batched checkpointed adjoint gradients vs the plain one-shot-per-launch form.
+
+    16 shots on one 256^3 grid (dx 10 m), O8 FP32, 2000 steps, Ricker f0 10 Hz, 20-point
+    sponge, receivers on the surface plane i1 = 1 every 4th point in i2 and i3, sources at seeded
+    surface positions; observed data from the background model with a 5 % Gaussian anomaly of
+    the squared slowness (sigma 10 points, centre); gradient of 1/2 |d - dobs|^2 with respect to
+    the squared slowness at the background; checkpoints every 45 steps. Batched: all shots in
+    each launch, the whole gradient (forward, then segment-wise recompute, adjoint and
+    gradient) replayed from one CUDA graph. Plain: the same kernels one shot per launch, from
+    the host, no graph. Both give bit-identical gradients (checked)."""
+    import numpy as np
+    import torch
+
+    from hpcscan_b200.grid import init_device
+    from hpcscan_b200.modeling import Batch, Shot, grf_velocity, run_graph, stable_dt
+
+    n = a.size if a.size != 512 else 256
+    nshot = a.shots or 16
+    nt = a.nt or 2000
+    order, dx, f0 = a.order, 10.0, 10.0
+    init_device(0)
+    dev = "cuda:0"
+    vel0 = grf_velocity((n, n, n), sigma=20.0, seed=1234)
+    c = (n - 1) / 2.0
+    ax = torch.arange(n, device=dev, dtype=torch.float32)
+    r2 = (ax[:, None, None] - c) ** 2 + (ax[None, :, None] - c) ** 2 + (ax[None, None, :] - c) ** 2
+    vel_true = vel0 / torch.sqrt(1.0 + 0.05 * torch.exp(-r2 / (2 * 10.0 ** 2)))
+    del r2
+    rec = np.array([(1, j, k) for j in range(0, n, 4) for k in range(0, n, 4)])
+    srcs = _surface_shots(n, nshot, 4321)
+    dt = stable_dt(order, dx, 4500.0)
+
+    def shots(vel, dobs=None):
+        return [Shot(n=(n, n, n), dx=dx, vel=vel, src=s, rec=rec, amp=1.0, sponge=20,
+                     dobs=None if dobs is None else dobs[i]) for i, s in enumerate(srcs)]
+
+    obs = Batch(shots(vel_true), order, dt, nt, f0)
+    obs.forward()
+    torch.cuda.synchronize()
+    dobs = [obs.traces(i).clone() for i in range(nshot)]
+    obs.close()
+    del obs
+    torch.cuda.empty_cache()
+
+    # batched: one graph for the whole gradient of all shots
+    bat = Batch(shots(vel0, dobs), order, dt, nt, f0, gradient=True, checkpoint=a.checkpoint)
+    mem_batched = torch.cuda.memory_allocated() / 1e9
+    ctas = bat.ctas_per_pass
+    g = run_graph(lambda s: (bat.forward(s), bat.backward(s)))
+    t_batched = _timed(g.replay, reps=1)          # warm-up replay
+    t_batched = _timed(g.replay, reps=1)
+    launches = bat.launches
+    grads = [bat.states[i].grad.clone() for i in range(nshot)]
+    J = [bat.misfit(i) for i in range(nshot)]
+    del g
+    bat.close()
+    del bat
+    torch.cuda.empty_cache()
+
+    # plain: one shot per launch, eager, shot after shot; each shot's set-up (allocation, tensor
+    # maps) stays outside the timed part, which is its forward + backward pass
+    def plain_one(i):
+        b = Batch(shots(vel0, dobs)[i:i + 1], order, dt, nt, f0, gradient=True,
+                  checkpoint=a.checkpoint)
+        sec = _timed(lambda: (b.forward(), b.backward()))
+        out = b.states[0].grad.clone()
+        b.close()
+        return sec, out
+    plain_one(0)                                   # warm-up
+    t_plain, same = 0.0, True
+    for i in range(nshot):
+        sec, gi = plain_one(i)
+        t_plain += sec
+        same = same and bool(torch.equal(gi, grads[i]))
+
+    pts = n ** 3
+    k = a.checkpoint
+    nck = (nt + k - 1) // k
+    # algorithmic bytes per shot: forward 16 B/pt-step, recompute 16 B, adjoint 16 B, gradient
+    # 20 B; checkpoint save (8 B/pt written) and restore (8 B read + 8 B written) per checkpoint
+    alg = pts * (16 * nt + 16 * (nt - nck) + 16 * nt + 20 * nt + 24 * nck) * nshot
+    peak, peak_src = measured_peak()
+    line = {
+        "metric": f"adjoint gradient shots/s ({n}^3, O{order} FP32, {nt} steps, checkpoint {k})",
+        "value": round(nshot / t_batched, 4), "unit": "shots/s", "n_gpus": 1, "steps": nt,
+        "warmup": 1, "ms_per_step": round(t_batched / nt * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian-random-field velocity 1500-4500 m/s, 5 % Gaussian "
+                "anomaly of the squared slowness, Ricker 10 Hz sources); no dataset involved",
+        "config": {"workload": "batched checkpointed adjoint gradients", "n": n, "shots": nshot,
+                   "order": order, "dx_m": dx, "receivers": len(rec), "sponge": 20,
+                   "checkpoint_every": k, "ctas_per_pass": ctas,
+                   "device_memory_gb": round(mem_batched, 1)},
+        "plain": {"value": round(nshot / t_plain, 4), "unit": "shots/s",
+                  "form": "same kernels, one shot per launch, eager host loop, no CUDA graph "
+                          "(per-shot set-up not timed)",
+                  "seconds": round(t_plain, 3)},
+        "speedup_vs_plain": round(t_plain / t_batched, 3),
+        "gradients_identical_to_plain": same,
+        "misfit_mean": float(np.mean(J)),
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": round(alg / t_batched / 1e9, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(alg / t_batched / 1e9 / peak, 4),
+                     "peak_source": peak_src,
+                     "alg_bytes": "per shot-step: 16 forward + 16 recompute + 16 adjoint + 20 "
+                                  "gradient, plus checkpoint save/restore"},
+        "seconds": round(t_batched, 3),
+    }
+    print(json.dumps(line))
+
+
+def modeling_arm(a):
+    """Batched multi-shot forward modelling: 64 shots on uneven cubes N_s = 128 + round(192 s /
+    63) (128 .. 320), dx 10 m, Gaussian-random-field velocity 1500-4500 m/s (seed 1234 + s,
+    Gaussian kernel sigma 20 points), Ricker 10 Hz point source at the surface centre (i1 = 1),
+    20-point sponge, O8 FP32, 1500 steps; every step of every shot in one launch, the time loop
+    in one CUDA graph; against the same kernels one shot per launch without a graph."""
+    import numpy as np
+    import torch
+
+    from hpcscan_b200.grid import init_device
+    from hpcscan_b200.modeling import Batch, Shot, grf_velocity, run_graph, stable_dt
+
+    nshot = a.shots or 64
+    nt = a.nt or 1500
+    order, dx, f0 = a.order, 10.0, 10.0
+    init_device(0)
+    sizes = [128 + round(192 * s / max(nshot - 1, 1)) for s in range(nshot)]
+    dt = stable_dt(order, dx, 4500.0)
+    shots = []
+    for s, n in enumerate(sizes):
+        vel = grf_velocity((n, n, n), sigma=20.0, seed=1234 + s)
+        rec = np.array([(1, j, n // 2) for j in range(0, n, 2)])
+        shots.append(Shot(n=(n, n, n), dx=dx, vel=vel, src=(1, n // 2, n // 2), rec=rec,
+                          amp=1.0, sponge=20))
+    bat = Batch(shots, order, dt, nt, f0)
+    g = run_graph(lambda st: bat.forward(st))
+    _timed(g.replay)
+    t_batched = _timed(g.replay)
+    traces = [bat.traces(i).clone() for i in range(nshot)]
+    launches = bat.launches // 2
+    del g
+    bat.close()
+    del bat
+    torch.cuda.empty_cache()
+    same, t_plain = True, 0.0
+    for i in range(nshot):
+        b = Batch(shots[i:i + 1], order, dt, nt, f0)
+        t_plain += _timed(b.forward)
+        same = same and bool(torch.equal(b.traces(0), traces[i]))
+        b.close()
+    pts = sum(n ** 3 for n in sizes) * nt
+    peak, peak_src = measured_peak()
+    line = {
+        "metric": f"batched modelling GPoint/s ({nshot} shots 128^3..320^3, O{order} FP32, {nt} steps)",
+        "value": round(pts / t_batched / 1e9, 4), "unit": "GPoint/s", "n_gpus": 1, "steps": nt,
+        "warmup": 1, "ms_per_step": round(t_batched / nt * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian-random-field velocities); no dataset involved",
+        "config": {"workload": "batched multi-shot modelling, one CUDA graph", "shots": nshot,
+                   "sizes": [sizes[0], sizes[-1]], "order": order, "dx_m": dx, "sponge": 20},
+        "shots_per_s": round(nshot / t_batched, 4),
+        "plain": {"value": round(pts / t_plain / 1e9, 4), "unit": "GPoint/s",
+                  "form": "same kernels, one shot per launch, eager host loop, no CUDA graph "
+                          "(per-shot set-up not timed)",
+                  "seconds": round(t_plain, 3)},
+        "speedup_vs_plain": round(t_plain / t_batched, 3),
+        "traces_identical_to_plain": same,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": round(16 * pts / t_batched / 1e9, 1),
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(16 * pts / t_batched / 1e9 / peak, 4), "peak_source": peak_src},
+        "seconds": round(t_batched, 3),
+    }
+    print(json.dumps(line))
+
+
 def main():
     a = parse_args()
+    if a.workload != "propa":
+        rank, world, _ = dist_env()
+        if a.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
+                                  "adjoint and no batched modelling path"}))
+            return
+        if world > 1 and rank != 0:
+            return
+        (adjoint_arm if a.workload == "adjoint" else modeling_arm)(a)
+        return
     if a.impl == "reference":
         reference_arm(a)
     else:

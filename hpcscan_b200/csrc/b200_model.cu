@@ -46,32 +46,31 @@ __device__ __forceinline__ float damping(const MShot& m, int64_t ii)
 	return m.g1[x] * (m.g2[y] * m.g3[z]);
 }
 
-// Source injection into slot `slot` of every shot, then the receivers of that slot into row n.
-__global__ void k_model_source_record(const MShot* __restrict__ shots, int n, int slot)
+// The receivers of slot `slot` of every shot into row n of its traces (the source was added by
+// the stencil pass). Grid (shots, receiver blocks), one thread per receiver.
+__global__ void k_model_record(const MShot* __restrict__ shots, int n, int slot)
 {
 	const MShot& m = shots[blockIdx.x];
-	float* p = m.wave + slot * m.field;
-	if (threadIdx.x == 0) {
-		const float g = damping(m, m.src);
-		p[m.src] = fmaf(g * m.amp, m.wavelet[n], p[m.src]);
-	}
-	__syncthreads();
-	for (int r = threadIdx.x; r < m.nrec; r += blockDim.x)
-		m.traces[(int64_t)n * m.nrec + r] = p[m.rec[r]];
+	const int r = blockIdx.y * blockDim.x + threadIdx.x;
+	if (r >= m.nrec) return;
+	m.traces[(int64_t)n * m.nrec + r] = m.wave[slot * m.field + m.rec[r]];
 }
 
-// Residual injection d[k] - dobs[k] (row k - 1) into adjoint slot `slot` at the receivers.
+// Residual injection d[k] - dobs[k] (row k - 1) into adjoint slot `slot` at the (distinct)
+// receivers. Grid (shots, receiver blocks).
 __global__ void k_model_residual(const MShot* __restrict__ shots, int k, int slot)
 {
 	const MShot& m = shots[blockIdx.x];
+	const int r = blockIdx.y * blockDim.x + threadIdx.x;
+	if (r >= m.nrec) return;
 	float* w = m.adj + slot * m.field;
 	const int64_t row = (int64_t)(k - 1) * m.nrec;
-	for (int r = threadIdx.x; r < m.nrec; r += blockDim.x) {
-		const int64_t ii = m.rec[r];
-		const float res = m.traces[row + r] - m.dobs[row + r];
-		w[ii] = fmaf(m.coef[ii] * damping(m, ii), res, w[ii]);
-	}
+	const int64_t ii = m.rec[r];
+	const float res = m.traces[row + r] - m.dobs[row + r];
+	w[ii] = fmaf(m.coef[ii] * damping(m, ii), res, w[ii]);
 }
+
+constexpr int kRecThreads = 128;
 
 // Stencil passes: R and the tile shape (shape 0), FP32 with fused multiply-adds.
 template <int R, int MODE>
@@ -88,6 +87,7 @@ struct b200_batch {
 	int nshot = 0;
 	int nslot = 0;
 	int ctas = 0;                   // CTAs of one stencil pass over the whole batch
+	int max_nrec = 0;
 	int smem[3] = {0, 0, 0};
 	ZShot* d_fwd = nullptr;         // stencil tables: forward, adjoint, gradient
 	ZShot* d_adj = nullptr;
@@ -106,6 +106,29 @@ int batch_tables(b200_batch* b, const b200_shot* shots, double dt, std::vector<Z
 	using CG = ModelCfg<R, MODE_GRAD>;
 	static_assert(CF::TX == CG::TX && CF::TY == CG::TY && CF::BX == CG::BX && CF::BY == CG::BY,
 			"one tiling for every pass");
+	int rc0 = cuda_error(cudaFuncSetAttribute(k_zmarch_batch<CF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			CF::SMEM), "cudaFuncSetAttribute(k_zmarch_batch)");
+	if (!rc0)
+		rc0 = cuda_error(cudaFuncSetAttribute(k_zmarch_batch<CG>,
+				cudaFuncAttributeMaxDynamicSharedMemorySize, CG::SMEM),
+				"cudaFuncSetAttribute(k_zmarch_batch)");
+	if (rc0) return rc0;
+	// one z-chunk for the batch: the longest (fewest halo re-reads) that still gives at least
+	// four waves of resident CTAs over all shots
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zmarch_batch<CF>, CF::NT, CF::SMEM);
+	const int64_t resident = (int64_t)(per_sm > 0 ? per_sm : 1) * num_sms();
+	int chunk = 128;
+	for (; chunk > 16; chunk /= 2) {
+		int64_t total = 0;
+		for (int i = 0; i < b->nshot; i++) {
+			const b200_layout* l = &shots[i].lay;
+			const int64_t x0 = l->s1 / CF::VX * CF::VX;
+			total += ((l->e1 + 1 - x0 + CF::TX - 1) / CF::TX) * ((l->e2 - l->s2 + CF::TY) / CF::TY) *
+			         ((l->e3 - l->s3 + chunk) / chunk);
+		}
+		if (total >= 4 * resident) break;
+	}
 	int cta = 0;
 	for (int i = 0; i < b->nshot; i++) {
 		const b200_shot& sh = shots[i];
@@ -129,10 +152,18 @@ int batch_tables(b200_batch* b, const b200_shot* shots, double dt, std::vector<Z
 		a.g2 = sh.sponge[1];
 		a.g3 = sh.sponge[2];
 		a.kscale = (float)(-1.0 / (dt * dt));
+		{
+			const int64_t sz = sh.src / (lay->n1 * lay->n2), sr = sh.src - sz * lay->n1 * lay->n2;
+			a.src_z = (int)sz;
+			a.src_y = (int)(sr / lay->n1);
+			a.src_x = (int)(sr - (sr / lay->n1) * lay->n1);
+			a.src_amp = sh.amp;
+			a.wavelet = sh.wavelet;
+		}
 		z.ntx = (a.e1 + 1 - a.x_start + CF::TX - 1) / CF::TX;
 		z.nty = (a.e2 - a.s2 + 1 + CF::TY - 1) / CF::TY;
 		const int nz = a.e3 - a.s3 + 1;
-		a.nz_chunk = nz < 64 ? nz : 64;
+		a.nz_chunk = nz < chunk ? nz : chunk;
 		z.nzc = (nz + a.nz_chunk - 1) / a.nz_chunk;
 		z.cta_begin = cta;
 		cta += z.ntx * z.nty * z.nzc;
@@ -175,31 +206,31 @@ int batch_tables(b200_batch* b, const b200_shot* shots, double dt, std::vector<Z
 	b->smem[0] = CF::SMEM;
 	b->smem[1] = CF::SMEM;
 	b->smem[2] = CG::SMEM;
-	int rc = cuda_error(cudaFuncSetAttribute(k_zmarch_batch<CF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			CF::SMEM), "cudaFuncSetAttribute(k_zmarch_batch)");
-	if (!rc)
-		rc = cuda_error(cudaFuncSetAttribute(k_zmarch_batch<CG>,
-				cudaFuncAttributeMaxDynamicSharedMemorySize, CG::SMEM),
-				"cudaFuncSetAttribute(k_zmarch_batch)");
-	return rc;
+	return B200_OK;
 }
 
 template <int R, int MODE>
-int launch_pass(const b200_batch* b, const ZShot* table, int su, int sp0, int sout, cudaStream_t s)
+int launch_pass(const b200_batch* b, const ZShot* table, int su, int sp0, int sout, int step,
+		cudaStream_t s)
 {
 	using Cfg = ModelCfg<R, MODE>;
-	k_zmarch_batch<Cfg><<<b->ctas, Cfg::NT, Cfg::SMEM, s>>>(table, b->nshot, su, sp0, sout);
+	k_zmarch_batch<Cfg><<<b->ctas, Cfg::NT, Cfg::SMEM, s>>>(table, b->nshot, su, sp0, sout, step);
 	return check_launch("k_zmarch_batch");
 }
 
 int dispatch_pass(const b200_batch* b, int mode, const ZShot* table, int su, int sp0, int sout,
-		cudaStream_t s)
+		int step, cudaStream_t s)
 {
 	return dispatch_order(2 * b->R, [&](auto rt) {
 		constexpr int R = decltype(rt)::value;
-		if (mode == MODE_GRAD) return launch_pass<R, MODE_GRAD>(b, table, su, sp0, sout, s);
-		return launch_pass<R, MODE_MODEL>(b, table, su, sp0, sout, s);
+		if (mode == MODE_GRAD) return launch_pass<R, MODE_GRAD>(b, table, su, sp0, sout, -1, s);
+		return launch_pass<R, MODE_MODEL>(b, table, su, sp0, sout, step, s);
 	});
+}
+
+dim3 rec_grid(const b200_batch* b)
+{
+	return dim3((unsigned)b->nshot, (unsigned)((b->max_nrec + kRecThreads - 1) / kRecThreads));
 }
 
 int check_shot(const b200_shot& sh, int order, bool need_adj, bool need_grad, int i)
@@ -271,6 +302,7 @@ int b200_batch_create(b200_batch** out, int order, int nslot, int nshot, const b
 		m.rec = sh.rec;
 		m.traces = sh.traces;
 		m.dobs = sh.dobs;
+		if (sh.nrec > b->max_nrec) b->max_nrec = sh.nrec;
 	}
 	auto upload = [&](auto** dst, const auto& v) -> int {
 		if (v.empty()) return B200_OK;
@@ -310,9 +342,10 @@ int b200_batch_forward_step(b200_batch* b, int n, int scur, int sprev, int sout,
 		return set_error(B200_ERR_ARG, "forward slots %d %d %d of %d", scur, sprev, sout, b->nslot);
 	if (n < 0) return set_error(B200_ERR_ARG, "step %d", n);
 	cudaStream_t s = as_stream(stream);
-	if (int rc = dispatch_pass(b, MODE_MODEL, b->d_fwd, scur, sprev, sout, s)) return rc;
-	k_model_source_record<<<b->nshot, 256, 0, s>>>(b->d_m, n, sout);
-	return check_launch("k_model_source_record");
+	if (int rc = dispatch_pass(b, MODE_MODEL, b->d_fwd, scur, sprev, sout, n, s)) return rc;
+	if (b->max_nrec == 0) return B200_OK;
+	k_model_record<<<rec_grid(b), kRecThreads, 0, s>>>(b->d_m, n, sout);
+	return check_launch("k_model_record");
 }
 
 int b200_batch_adjoint_step(b200_batch* b, int k, int scur, void* stream)
@@ -321,8 +354,9 @@ int b200_batch_adjoint_step(b200_batch* b, int k, int scur, void* stream)
 	if (scur < 0 || scur > 1 || k < 1) return set_error(B200_ERR_ARG, "adjoint step %d slot %d", k, scur);
 	cudaStream_t s = as_stream(stream);
 	const int o = 1 - scur;
-	if (int rc = dispatch_pass(b, MODE_MODEL, b->d_adj, scur, o, o, s)) return rc;
-	k_model_residual<<<b->nshot, 256, 0, s>>>(b->d_m, k, o);
+	if (int rc = dispatch_pass(b, MODE_MODEL, b->d_adj, scur, o, o, -1, s)) return rc;
+	if (b->max_nrec == 0) return B200_OK;
+	k_model_residual<<<rec_grid(b), kRecThreads, 0, s>>>(b->d_m, k, o);
 	return check_launch("k_model_residual");
 }
 
@@ -331,7 +365,7 @@ int b200_batch_gradient(b200_batch* b, int swave, int sadj, void* stream)
 	if (!b || !b->has_grad) return set_error(B200_ERR_ARG, "batch without gradient");
 	if (swave < 0 || swave >= b->nslot || sadj < 0 || sadj > 1)
 		return set_error(B200_ERR_ARG, "gradient slots %d %d", swave, sadj);
-	return dispatch_pass(b, MODE_GRAD, b->d_grad, swave, sadj, 0, as_stream(stream));
+	return dispatch_pass(b, MODE_GRAD, b->d_grad, swave, sadj, 0, -1, as_stream(stream));
 }
 
 int b200_batch_info(const b200_batch* b, int* ctas_per_pass)

@@ -219,6 +219,9 @@ struct ZArgs {
 	const float* g3;
 	float kscale;
 	int64_t out_slot_stride;   // elements between slots of the output grid
+	int src_x, src_y, src_z;   // point source of MODE_MODEL (added when the step is >= 0)
+	float src_amp;
+	const float* wavelet;
 };
 
 
@@ -243,7 +246,7 @@ struct Ring {
 template <class Cfg, bool SLOTS>
 __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUtensorMap* tm_p0,
 		const CUtensorMap* tm_p1, const CUtensorMap* tm_p2, const ZArgs<typename Cfg::C>& a,
-		int bx, int by, int bz, int slot_u, int slot_p0, int slot_out)
+		int bx, int by, int bz, int slot_u, int slot_p0, int slot_out, int step)
 {
 	using S = typename Cfg::Stor;
 	using C = typename Cfg::C;
@@ -589,6 +592,11 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 								const float2 t = A2::mac(A2::add(pc, pc), cf, lap);
 								const float2 gg = A2::mul(G, G);
 								r2 = A2::mac(A2::mul(make_float2(-gg.x, -gg.y), pm), G, t);
+								if (step >= 0 && k == a.src_z && Y0 + v == a.src_y) {
+									// the point source: p+(src) += G amp wavelet[step]
+									if (X + e == a.src_x) r2.x = fmaf(G.x * a.src_amp, a.wavelet[step], r2.x);
+									if (X + e + 1 == a.src_x) r2.y = fmaf(G.y * a.src_amp, a.wavelet[step], r2.y);
+								}
 							} else if constexpr (Cfg::MODE == MODE_GRAD) {
 								// g += k C w Lap p
 								const int o = (yl + v) * TX + xl + e;
@@ -702,7 +710,7 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch(
 		const ZArgs<typename Cfg::C> a)
 {
 	zmarch_body<Cfg, false>(&tm_u, &tm_prn, &tm_coef, &tm_coef, a, (int)blockIdx.x,
-			(int)blockIdx.y, (int)blockIdx.z, 0, 0, 0);
+			(int)blockIdx.y, (int)blockIdx.z, 0, 0, 0, -1);
 }
 
 // One shot of a batched launch: its tensor maps (slotted grids: u, pointwise tiles 0..2), its
@@ -716,7 +724,7 @@ struct alignas(64) ZShot {
 // Every shot of a batch in one launch: CTA b works on the shot whose range holds b.
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch_batch(const ZShot* __restrict__ shots,
-		int nshot, int slot_u, int slot_p0, int slot_out)
+		int nshot, int slot_u, int slot_p0, int slot_out, int step)
 {
 	const int b = (int)blockIdx.x;
 	int s = 0;
@@ -725,7 +733,7 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch_batch(const ZShot
 	const int local = b - sh.cta_begin;
 	const int bx = local % sh.ntx, by = (local / sh.ntx) % sh.nty, bz = local / (sh.ntx * sh.nty);
 	zmarch_body<Cfg, true>(&sh.tm[0], &sh.tm[1], &sh.tm[2], &sh.tm[3], sh.a, bx, by, bz, slot_u,
-			slot_p0, slot_out);
+			slot_p0, slot_out, step);
 }
 
 }  // namespace
