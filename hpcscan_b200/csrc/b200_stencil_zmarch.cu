@@ -144,7 +144,7 @@ int make_map_slots(CUtensorMap* m, const void* base, const b200_layout* lay, int
 bool zmarch_accepts(const b200_layout* lay, int dtype)
 {
 	if (lay->dim != 3) return false;
-	if (dtype != B200_F32 && dtype != B200_F64) return false;
+	if (dtype != B200_F32 && dtype != B200_F64 && dtype != B200_F16 && dtype != B200_BF16) return false;
 	if ((lay->n1 * dtype_size(dtype)) % 16 != 0) return false;   // TMA stride rule
 	if (lay->n1 > (1 << 30) || lay->n2 > (1 << 30) || lay->n3 > (1 << 30)) return false;
 	return true;
@@ -162,9 +162,13 @@ int run_zmarch(int mode, const b200_layout* lay, int order, const b200_field& in
 				lay->e3 - lay->s3 + 1 < lay->halo + 2)
 			return B200_OK;
 	}
+	const bool half = in.dtype == B200_F16 || in.dtype == B200_BF16;
+	if (half && mode != MODE_PRESSURE) return B200_OK;      // 16-bit: the pressure update only
+	if (out.dtype != in.dtype) return B200_OK;
 	if ((reinterpret_cast<uintptr_t>(in.data) | reinterpret_cast<uintptr_t>(out.data)) % 16) return B200_OK;
 	if (coef) {
-		if (coef->dtype != in.dtype) return B200_OK;
+		if (coef->dtype != in.dtype && !(half && coef->dtype == B200_F32)) return B200_OK;
+		if (coef->dtype == B200_F32 && (lay->n1 * 4) % 16) return B200_OK;
 		if (reinterpret_cast<uintptr_t>(coef->data) % 16) return B200_OK;
 	}
 	const bool exact = !has_shapes(mode) || g_arith == B200_ARITH_EXACT;

@@ -153,13 +153,68 @@ __device__ __forceinline__ void lds_vec(const S* p, C* out)
 	}
 }
 
+// The register queue along i3: the compute type per point, or, for 16-bit storage, the stored
+// values two per register (half the registers; converted to FP32 where the stencil uses them).
+template <typename S, typename C> struct ZQueue {
+	using T = C;
+	static constexpr int W = 1;
+	static __device__ __forceinline__ C get(const T* row, int e) { return row[e]; }
+	static __device__ __forceinline__ float2 get2(const T* row, int e)
+	{
+		return make_float2((float)row[e], (float)row[e + 1]);
+	}
+	template <int N>
+	static __device__ __forceinline__ void push(const S* p, T* row) { lds_vec<S, C, N>(p, row); }
+};
+template <> struct ZQueue<__half, float> {
+	using T = __half2;
+	static constexpr int W = 2;
+	static __device__ __forceinline__ float get(const T* row, int e)
+	{
+		return (e & 1) ? __high2float(row[e >> 1]) : __low2float(row[e >> 1]);
+	}
+	static __device__ __forceinline__ float2 get2(const T* row, int e) { return __half22float2(row[e >> 1]); }
+	template <int N>
+	static __device__ __forceinline__ void push(const __half* p, T* row)
+	{
+#pragma unroll
+		for (int b = 0; b < N / 8; b++) {
+			const uint4 raw = reinterpret_cast<const uint4*>(p)[b];
+			const T* v = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+			for (int i = 0; i < 4; i++) row[b * 4 + i] = v[i];
+		}
+	}
+};
+template <> struct ZQueue<__nv_bfloat16, float> {
+	using T = __nv_bfloat162;
+	static constexpr int W = 2;
+	static __device__ __forceinline__ float get(const T* row, int e)
+	{
+		return (e & 1) ? __high2float(row[e >> 1]) : __low2float(row[e >> 1]);
+	}
+	static __device__ __forceinline__ float2 get2(const T* row, int e) { return __bfloat1622float2(row[e >> 1]); }
+	template <int N>
+	static __device__ __forceinline__ void push(const __nv_bfloat16* p, T* row)
+	{
+#pragma unroll
+		for (int b = 0; b < N / 8; b++) {
+			const uint4 raw = reinterpret_cast<const uint4*>(p)[b];
+			const T* v = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+			for (int i = 0; i < 4; i++) row[b * 4 + i] = v[i];
+		}
+	}
+};
+
 constexpr int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // ---- kernel configuration -----------------------------------------------------------------------
 template <typename S, int R_, int MODE_, int TX_, int TY_, int VY_, int PF_, bool EXACT_ = true,
-		int MINB_ = 0>
+		int MINB_ = 0, typename SC_ = S>
 struct ZCfg {
 	using Stor = S;
+	using CoefStor = SC_;                                    // coef storage (FP32 with 16-bit waves)
 	using C = typename Storage<S>::C;
 	static constexpr bool EXACT = EXACT_;
 	static constexpr int R = R_;
@@ -185,11 +240,16 @@ struct ZCfg {
 	static constexpr int U_STRIDE = round_up(U_BYTES, 128);
 	static constexpr int PT_BYTES = TX * TY * (int)sizeof(S);
 	static constexpr int PT_STRIDE = round_up(PT_BYTES, 128);
+	static constexpr int CT_BYTES = TX * TY * (int)sizeof(SC_);
+	static constexpr int CT_STRIDE = round_up(CT_BYTES, 128);
+	// one slot of the pointwise ring: output-plane tile, coef tile, third tile (gradient)
+	static constexpr int SLOT_P = PT_STRIDE + CT_STRIDE + (NPT > 2 ? PT_STRIDE : 0);
+	static constexpr int SLOT_TX = PT_BYTES + CT_BYTES + (NPT > 2 ? PT_BYTES : 0);
 	static constexpr int NTX = TX / VX;
 	static constexpr int NC = NTX * (TY / VY);              // consumer threads
 	static constexpr int NWC = NC / 32;                      // consumer warps
 	static constexpr int NT = NC + 32;                       // + one producer warp
-	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * NPT * PT_STRIDE : 0) +
+	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * SLOT_P : 0) +
 	                            (2 * NSU + 2 * NSP) * 8;
 	// CTAs per SM the launch bounds ask for (registers follow: an SM has four sub-partitions
 	// of 16K registers and spreads a CTA's warps over them). Two CTAs per SM for R <= 4 with
@@ -200,6 +260,7 @@ struct ZCfg {
 			"the modelling engine computes in FP32");
 	static_assert(BX <= 256 && BY <= 256, "TMA box limit");
 	static_assert((BX * sizeof(S)) % 16 == 0 && (TX * sizeof(S)) % 16 == 0, "TMA inner extent");
+	static_assert((TX * sizeof(SC_)) % 16 == 0, "TMA inner extent (coef)");
 };
 
 template <typename C>
@@ -249,6 +310,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 		int bx, int by, int bz, int slot_u, int slot_p0, int slot_out, int step)
 {
 	using S = typename Cfg::Stor;
+	using SC = typename Cfg::CoefStor;
 	using C = typename Cfg::C;
 	constexpr bool EX = Cfg::EXACT;
 	using A = Arith<EX>;
@@ -256,17 +318,16 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	constexpr int R4 = Cfg::R4, RY = Cfg::RY, RZ = Cfg::RZ, BX = Cfg::BX;
 	constexpr int NSU = Cfg::NSU, NSP = Cfg::NSP, NC = Cfg::NC;
 	constexpr int UE = Cfg::U_STRIDE / (int)sizeof(S);     // elements between input tiles
-	constexpr int PE = Cfg::PT_STRIDE / (int)sizeof(S);    // elements between prn/coef tiles
 	constexpr unsigned FULL = 0xffffffffu;
 
 	extern __shared__ unsigned char smem_raw[];
 	unsigned char* smem = reinterpret_cast<unsigned char*>(
 			(reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
 	S* su = reinterpret_cast<S*>(smem);
-	S* sp = reinterpret_cast<S*>(smem + NSU * Cfg::U_STRIDE);
+	unsigned char* sp = smem + NSU * Cfg::U_STRIDE;       // pointwise ring, Cfg::SLOT_P per slot
 	constexpr int NPT = Cfg::NPT;
 	uint64_t* bars = reinterpret_cast<uint64_t*>(
-			smem + NSU * Cfg::U_STRIDE + (Cfg::P ? NSP * NPT * Cfg::PT_STRIDE : 0));
+			smem + NSU * Cfg::U_STRIDE + (Cfg::P ? NSP * Cfg::SLOT_P : 0));
 	uint64_t* full_u = bars;
 	uint64_t* empty_u = bars + NSU;
 	uint64_t* full_p = bars + 2 * NSU;
@@ -329,13 +390,13 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						ok = false;
 						break;
 					}
-					mbar_arrive_expect_tx(&full_p[wp.slot], NPT * Cfg::PT_BYTES);
-					tma_tile<SLOTS>(sp + (NPT * wp.slot) * PE, tm_p0, tile_x0, tile_y0, z0 + o,
-							slot_p0, &full_p[wp.slot]);
-					tma_tile<SLOTS>(sp + (NPT * wp.slot + 1) * PE, tm_p1, tile_x0, tile_y0, z0 + o, 0,
+					unsigned char* slot = sp + wp.slot * Cfg::SLOT_P;
+					mbar_arrive_expect_tx(&full_p[wp.slot], Cfg::SLOT_TX);
+					tma_tile<SLOTS>(slot, tm_p0, tile_x0, tile_y0, z0 + o, slot_p0, &full_p[wp.slot]);
+					tma_tile<SLOTS>(slot + Cfg::PT_STRIDE, tm_p1, tile_x0, tile_y0, z0 + o, 0,
 							&full_p[wp.slot]);
 					if constexpr (NPT > 2)
-						tma_tile<SLOTS>(sp + (NPT * wp.slot + 2) * PE, tm_p2, tile_x0, tile_y0,
+						tma_tile<SLOTS>(slot + Cfg::PT_STRIDE + Cfg::CT_STRIDE, tm_p2, tile_x0, tile_y0,
 								z0 + o, 0, &full_p[wp.slot]);
 					issued_p = o + 1;
 					wp.advance();
@@ -359,7 +420,9 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	const int yl = (tid / Cfg::NTX) * VY;
 	const int X = tile_x0 + xl;
 	const int Y0 = tile_y0 + yl;
-	C q[2 * RZ + 1][VY][VX];           // values along i3 of this thread's points
+	using Q = ZQueue<S, C>;
+	constexpr int VQ = VX / Q::W;
+	typename Q::T q[2 * RZ + 1][VY][VQ];   // values along i3 of this thread's points
 	// `alive` turns false when a bounded wait runs out: the warp then skips all work but keeps
 	// the loop's barrier sequence, so no other warp is left waiting at a named barrier.
 	bool alive = true;
@@ -449,11 +512,11 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 #pragma unroll
 					for (int v = 0; v < VY; v++)
 #pragma unroll
-						for (int e = 0; e < VX; e++) q[i][v][e] = q[i + 1][v][e];
+						for (int e = 0; e < VQ; e++) q[i][v][e] = q[i + 1][v][e];
 				const S* t = su + s * UE;
 #pragma unroll
 				for (int v = 0; v < VY; v++)
-					lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl, q[2 * RZ][v]);
+					Q::template push<VX>(t + (yl + v + RY) * BX + R4 + xl, q[2 * RZ][v]);
 				if constexpr (Cfg::BC) {
 					// values after the boundary condition: boundary lines and planes are zero; a
 					// z-halo plane (loaded from its mirror) is minus the mirror after the i1/i2
@@ -480,11 +543,16 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 			const int k = z0 + o;                     // output plane
 			const int sc = Cfg::ZQ ? rc.slot : s;      // slot holding plane k with its halos
 			const S* t = su + sc * UE;
-			const S* pt = nullptr;
+			const S* pt = nullptr;     // output-plane tile (prn, or w for the gradient)
+			const SC* ct = nullptr;    // coef tile
+			const S* gt = nullptr;     // gradient tile
 			if constexpr (Cfg::P) {
 				if (alive && !__all_sync(FULL, mbar_wait(&full_p[rp.slot], rp.phase, deadline)))
 					alive = false;
-				pt = sp + (NPT * rp.slot) * PE;
+				unsigned char* slot = sp + rp.slot * Cfg::SLOT_P;
+				pt = reinterpret_cast<const S*>(slot);
+				ct = reinterpret_cast<const SC*>(slot + Cfg::PT_STRIDE);
+				gt = reinterpret_cast<const S*>(slot + Cfg::PT_STRIDE + Cfg::CT_STRIDE);
 			}
 			const bool kb = Cfg::BC && (k == a.s3 || k == a.e3);
 			if constexpr (Cfg::BC) {
@@ -523,15 +591,15 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 				// rows of this thread's columns, plane k: (VY + 2 RY) x VX values (near a
 				// boundary the centre rows come from the patched tile too: a thread's vector
 				// can straddle the last inner point, and its halo part needs the patch)
-				C yv[VY + 2 * RY][VX];
+				typename Q::T yv[VY + 2 * RY][VQ];
 #pragma unroll
 				for (int r = 0; r < VY + 2 * RY; r++) {
 					const int v = r - RY;
 					if (v >= 0 && v < VY && Cfg::ZQ && !(Cfg::BC && (near || kb))) {
 #pragma unroll
-						for (int e = 0; e < VX; e++) yv[r][e] = q[RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
+						for (int e = 0; e < VQ; e++) yv[r][e] = q[RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
 					} else {
-						lds_vec<S, C, VX>(t + (yl + r) * BX + R4 + xl, yv[r]);
+						Q::template push<VX>(t + (yl + r) * BX + R4 + xl, yv[r]);
 					}
 				}
 #pragma unroll
@@ -544,7 +612,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						for (int h = 0; h < R4 / VX; h++)
 							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + xl + h * VX, &xv[h * VX]);
 #pragma unroll
-						for (int e = 0; e < VX; e++) xv[R4 + e] = yv[v + RY][e];
+						for (int e = 0; e < VX; e++) xv[R4 + e] = Q::get(yv[v + RY], e);
 #pragma unroll
 						for (int h = 0; h < R4 / VX; h++)
 							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl + VX + h * VX,
@@ -565,10 +633,10 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 									return make_float2(xv[R4 + e + kk], xv[R4 + e + 1 + kk]); }, i1);
 							if constexpr (Cfg::YH)
 								dy = d2_axis2<R, EX>([&](int kk) {
-									return make_float2(yv[v + RY + kk][e], yv[v + RY + kk][e + 1]); }, i2);
+									return Q::get2(yv[v + RY + kk], e); }, i2);
 							if constexpr (Cfg::ZQ)
 								dz = d2_axis2<R, EX>([&](int kk) {
-									return make_float2(q[RZ + kk][v][e], q[RZ + kk][v][e + 1]); }, i3);
+									return Q::get2(q[RZ + kk][v], e); }, i3);
 							if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
 								r2 = dx;
 							} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
@@ -585,9 +653,9 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 										a.g1[min(X + e + 1, a.e1)] * gyz);
 								const int o = (yl + v) * TX + xl + e;
 								const float2 pm = make_float2(Storage<S>::load(pt[o]), Storage<S>::load(pt[o + 1]));
-								const float2 cf = make_float2(Storage<S>::load(pt[PE + o]),
-										Storage<S>::load(pt[PE + o + 1]));
-								const float2 pc = make_float2(yv[v + RY][e], yv[v + RY][e + 1]);
+								const float2 cf = make_float2(Storage<SC>::load(ct[o]),
+										Storage<SC>::load(ct[o + 1]));
+								const float2 pc = Q::get2(yv[v + RY], e);
 								const float2 lap = A2::add(A2::add(dx, dy), dz);
 								const float2 t = A2::mac(A2::add(pc, pc), cf, lap);
 								const float2 gg = A2::mul(G, G);
@@ -601,23 +669,23 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 								// g += k C w Lap p
 								const int o = (yl + v) * TX + xl + e;
 								const float2 w = make_float2(Storage<S>::load(pt[o]), Storage<S>::load(pt[o + 1]));
-								const float2 cf = make_float2(Storage<S>::load(pt[PE + o]),
-										Storage<S>::load(pt[PE + o + 1]));
-								const float2 g0 = make_float2(Storage<S>::load(pt[2 * PE + o]),
-										Storage<S>::load(pt[2 * PE + o + 1]));
+								const float2 cf = make_float2(Storage<SC>::load(ct[o]),
+										Storage<SC>::load(ct[o + 1]));
+								const float2 g0 = make_float2(Storage<S>::load(gt[o]),
+										Storage<S>::load(gt[o + 1]));
 								const float2 kw = A2::mul(A2::mul(make_float2(a.kscale, a.kscale), cf), w);
 								r2 = A2::mac(g0, kw, A2::add(A2::add(dx, dy), dz));
 							} else {
 								float pn[2], cf[2];
 								pn[0] = Storage<S>::load(pt[(yl + v) * TX + xl + e]);
 								pn[1] = Storage<S>::load(pt[(yl + v) * TX + xl + e + 1]);
-								cf[0] = Storage<S>::load(pt[PE + (yl + v) * TX + xl + e]);
-								cf[1] = Storage<S>::load(pt[PE + (yl + v) * TX + xl + e + 1]);
+								cf[0] = Storage<SC>::load(ct[(yl + v) * TX + xl + e]);
+								cf[1] = Storage<SC>::load(ct[(yl + v) * TX + xl + e + 1]);
 								if (a.coef_scale != 1.0f) {
 									cf[0] = cf[0] * a.coef_scale;
 									cf[1] = cf[1] * a.coef_scale;
 								}
-								r2 = leapfrog2<EX>(make_float2(yv[v + RY][e], yv[v + RY][e + 1]),
+								r2 = leapfrog2<EX>(Q::get2(yv[v + RY], e),
 										make_float2(pn[0], pn[1]), make_float2(cf[0], cf[1]),
 										A2::add(A2::add(dx, dy), dz));
 							}
@@ -634,12 +702,12 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						if constexpr (Cfg::YH) {
 #pragma unroll
 							for (int e = 0; e < VX; e++)
-								dy[e] = d2_axis<C, R, EX>([&](int kk) { return yv[v + RY + kk][e]; }, a.inv2_2);
+								dy[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
 						}
 						if constexpr (Cfg::ZQ) {
 #pragma unroll
 							for (int e = 0; e < VX; e++)
-								dz[e] = d2_axis<C, R, EX>([&](int kk) { return q[RZ + kk][v][e]; }, a.inv2_3);
+								dz[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(q[RZ + kk][v], e); }, a.inv2_3);
 						}
 						if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
 #pragma unroll
@@ -656,12 +724,12 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						} else {
 							C pn[VX], cf[VX];
 							lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
-							lds_vec<S, C, VX>(pt + PE + (yl + v) * TX + xl, cf);
+							lds_vec<SC, C, VX>(ct + (yl + v) * TX + xl, cf);
 #pragma unroll
 							for (int e = 0; e < VX; e++) {
 								C c = cf[e];
 								if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
-								res[e] = leapfrog<C, EX>(yv[v + RY][e], pn[e], c,
+								res[e] = leapfrog<C, EX>(Q::get(yv[v + RY], e), pn[e], c,
 										A::add(A::add(dx[e], dy[e]), dz[e]));
 							}
 						}
@@ -837,6 +905,17 @@ int launch_shape(const ZLaunch& L)
 		return launch_zmarch<Cfg>(L);
 }
 
+// 16-bit wavefields (FP16 or BF16, with a per-field scale) computing in FP32 with fused
+// multiply-adds: one tile shape, 8 points per thread; coef in the same 16-bit type or FP32.
+template <int MODE, int R, typename S>
+int launch_16bit(const ZLaunch& L)
+{
+	constexpr int TY = R <= 4 ? 28 : 16;
+	if (L.coef && L.coef->dtype == B200_F32)
+		return launch_zmarch<ZCfg<S, R, MODE, 64, TY, 1, 2, false, 0, float>>(L);
+	return launch_zmarch<ZCfg<S, R, MODE, 64, TY, 1, 2, false, 0, S>>(L);
+}
+
 // Dispatch storage type, half width, shape and arithmetic for one operator. NSHAPES and
 // WITH_FMA bound the instantiations (the single-axis operators use shape 0, exact only).
 template <int MODE, int NSHAPES, bool WITH_FMA>
@@ -859,6 +938,10 @@ int launch_mode(const ZLaunch& L)
 			}
 			return set_error(B200_ERR_ARG, "stencil shape %d", shape);
 		};
+		if constexpr (MODE == MODE_PRESSURE) {
+			if (L.in->dtype == B200_F16) return launch_16bit<MODE, R, __half>(L);
+			if (L.in->dtype == B200_BF16) return launch_16bit<MODE, R, __nv_bfloat16>(L);
+		}
 		if (L.in->dtype == B200_F64) return go(double{});
 		return go(float{});
 	});
