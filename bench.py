@@ -58,7 +58,7 @@ def parse_args():
     p.add_argument("--cpu-steps", type=int, default=200,
                    help="time steps of the bounded reference CPU sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    p.add_argument("--workload", default="propa", choices=["propa", "adjoint", "modeling"],
+    p.add_argument("--workload", default="propa", choices=["propa", "adjoint", "modeling", "mixed"],
                    help="propa (default, the headline), adjoint (batched checkpointed gradients) "
                         "or modeling (batched uneven forward shots)")
     p.add_argument("--shots", type=int, default=0, help="shots (adjoint: 16, modeling: 64)")
@@ -644,6 +644,83 @@ def modeling_arm(a):
     print(json.dumps(line))
 
 
+def mixed_arm(a):
+    """Mixed-precision Propa: the eigen-mode test (ratioCFL 0.8, modes (1, 1, 1)) at 512^3 (or
+    --size), O8 (or --order), 1000 steps (or --nt), wavefields in FP16 and in BF16 with a
+    power-of-two per-field scale, FP32 coef and FP32 stencil arithmetic; against the FP64 run
+    of the same steps (bit-identical to the reference's FP64 build) and the analytic solution.
+    A step = boundary condition + pressure update, as in the headline workload."""
+    import numpy as np
+    import torch
+
+    from hpcscan_b200 import layout as L
+    from hpcscan_b200.grid import init_device
+    from hpcscan_b200.propagator import Propagator_Ac2, l1_sums_eigen
+
+    n, order = a.size, a.order
+    nt = a.nt or 1000
+    init_device(0)
+    results = {}
+    finals = {}
+    for prec, coef_prec, scale in (("f64", "f64", 1.0), ("f32", "f32", 1.0), ("f16", "f32", 2.0 ** 4),
+                                   ("bf16", "f32", 1.0)):
+        lay = L.b200_layout(3, n, n, n, order=order, prec=prec)
+        propa = Propagator_Ac2(lay, coef_prec=coef_prec, wave_scale=scale)
+        propa.initialize(ratio_cfl=0.8, nt=nt, snap_inc=max(1, nt // 10), modes=(1, 1, 1))
+        s = propa.setup
+        prn, prc = propa.prnGrid, propa.prcGrid
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sum1 = sum2 = np.float32(0.0)
+        kernel_ms = 0.0
+        for it in range(nt):
+            if it == 3:
+                torch.cuda.synchronize()
+                e0.record(stream)
+            propa.computeWavefieldNextTimeStep(prn, prc)
+            if it % s.snap_inc == 0:
+                amp = s.amplitude(s.time_of_step(it, "f64" if prec == "f64" else "f32"))
+                s1, s2 = l1_sums_eigen(prn, propa, amp)
+                sum1 = np.float32(sum1 + np.float32(s1))
+                sum2 = np.float32(sum2 + np.float32(s2))
+            prn, prc = prc, prn
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        steps = nt - 3
+        bpp = {"f64": 32, "f32": 16, "f16": 10, "bf16": 10}[prec]
+        finals[prec] = lay.inner(prc.to_numpy()).astype(np.float32)
+        results[prec] = {"gpoint_s": round(lay.inner_points * steps / sec / 1e9, 3),
+                         "ms_per_step": round(sec / steps * 1e3, 4),
+                         "alg_gb_s": round(bpp * lay.inner_points * steps / sec / 1e9, 1),
+                         "bytes_per_point": bpp,
+                         "err_test_case": float(sum1 / sum2), "wave_scale": scale,
+                         "coef": coef_prec}
+        del propa, prn, prc
+        torch.cuda.empty_cache()
+    ref = finals.pop("f64")
+    peak = float(np.linalg.norm(ref.astype(np.float64)))
+    for prec, f in finals.items():
+        d = (f.astype(np.float64) - ref.astype(np.float64)).ravel()
+        results[prec]["rel_l2_vs_fp64"] = float(np.linalg.norm(d) / peak)
+    pk, pk_src = measured_peak()
+    line = {
+        "metric": f"mixed-precision Propa GPoint/s (O{order}, FP16 wavefields, FP32 coef and "
+                  f"arithmetic, {n}^3, {nt} steps)",
+        "value": results["f16"]["gpoint_s"], "unit": "GPoint/s", "n_gpus": 1, "steps": nt - 3,
+        "warmup": 3, "ms_per_step": results["f16"]["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16 storage, f32 compute",
+        "data": "synthetic (eigen mode, the reference's Propa initialisation)",
+        "config": {"workload": "mixed-precision Propa (BC + pressure update per step)", "n": n,
+                   "order": order, "ratio_cfl": 0.8, "steps": nt},
+        "per_precision": results,
+        "roofline": {"bound": "hbm", "achieved": results["f16"]["alg_gb_s"], "peak": pk,
+                     "unit": "GB/s", "frac": round(results["f16"]["alg_gb_s"] / pk, 4),
+                     "peak_source": pk_src, "note": "whole step (BC + pressure), 10 B/point"},
+    }
+    print(json.dumps(line))
+
+
 def main():
     a = parse_args()
     if a.workload != "propa":
@@ -655,7 +732,7 @@ def main():
             return
         if world > 1 and rank != 0:
             return
-        (adjoint_arm if a.workload == "adjoint" else modeling_arm)(a)
+        {"adjoint": adjoint_arm, "modeling": modeling_arm, "mixed": mixed_arm}[a.workload](a)
         return
     if a.impl == "reference":
         reference_arm(a)
