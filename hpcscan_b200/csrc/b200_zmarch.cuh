@@ -624,6 +624,15 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						const float2 i1 = make_float2(a.inv2_1, a.inv2_1);
 						const float2 i2 = make_float2(a.inv2_2, a.inv2_2);
 						const float2 i3 = make_float2(a.inv2_3, a.inv2_3);
+						// the pointwise tiles of this row, one vector load each
+						constexpr int NV = Cfg::P ? VX : 1;
+						float pv0[NV], pv1[NV], pv2[(Cfg::MODE == MODE_GRAD) ? VX : 1];
+						if constexpr (Cfg::P) {
+							lds_vec<S, float, VX>(pt + (yl + v) * TX + xl, pv0);
+							lds_vec<SC, float, VX>(ct + (yl + v) * TX + xl, pv1);
+							if constexpr (Cfg::MODE == MODE_GRAD)
+								lds_vec<S, float, VX>(gt + (yl + v) * TX + xl, pv2);
+						}
 #pragma unroll
 						for (int pp = 0; pp < VX / 2; pp++) {
 							const int e = 2 * pp;
@@ -651,10 +660,8 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 								const float gyz = a.g2[min(Y0 + v, a.e2)] * a.g3[k];
 								const float2 G = make_float2(a.g1[min(X + e, a.e1)] * gyz,
 										a.g1[min(X + e + 1, a.e1)] * gyz);
-								const int o = (yl + v) * TX + xl + e;
-								const float2 pm = make_float2(Storage<S>::load(pt[o]), Storage<S>::load(pt[o + 1]));
-								const float2 cf = make_float2(Storage<SC>::load(ct[o]),
-										Storage<SC>::load(ct[o + 1]));
+								const float2 pm = make_float2(pv0[e], pv0[e + 1]);
+								const float2 cf = make_float2(pv1[e], pv1[e + 1]);
 								const float2 pc = Q::get2(yv[v + RY], e);
 								const float2 lap = A2::add(A2::add(dx, dy), dz);
 								const float2 t = A2::mac(A2::add(pc, pc), cf, lap);
@@ -667,20 +674,13 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 								}
 							} else if constexpr (Cfg::MODE == MODE_GRAD) {
 								// g += k C w Lap p
-								const int o = (yl + v) * TX + xl + e;
-								const float2 w = make_float2(Storage<S>::load(pt[o]), Storage<S>::load(pt[o + 1]));
-								const float2 cf = make_float2(Storage<SC>::load(ct[o]),
-										Storage<SC>::load(ct[o + 1]));
-								const float2 g0 = make_float2(Storage<S>::load(gt[o]),
-										Storage<S>::load(gt[o + 1]));
+								const float2 w = make_float2(pv0[e], pv0[e + 1]);
+								const float2 cf = make_float2(pv1[e], pv1[e + 1]);
+								const float2 g0 = make_float2(pv2[e], pv2[e + 1]);
 								const float2 kw = A2::mul(A2::mul(make_float2(a.kscale, a.kscale), cf), w);
 								r2 = A2::mac(g0, kw, A2::add(A2::add(dx, dy), dz));
 							} else {
-								float pn[2], cf[2];
-								pn[0] = Storage<S>::load(pt[(yl + v) * TX + xl + e]);
-								pn[1] = Storage<S>::load(pt[(yl + v) * TX + xl + e + 1]);
-								cf[0] = Storage<SC>::load(ct[(yl + v) * TX + xl + e]);
-								cf[1] = Storage<SC>::load(ct[(yl + v) * TX + xl + e + 1]);
+								float pn[2] = {pv0[e], pv0[e + 1]}, cf[2] = {pv1[e], pv1[e + 1]};
 								if (a.coef_scale != 1.0f) {
 									cf[0] = cf[0] * a.coef_scale;
 									cf[1] = cf[1] * a.coef_scale;
