@@ -78,6 +78,8 @@ SIGNATURES = {
     "b200_fill_const": [_PL, Field, _PB, _D, _VP],
     "b200_fill_separable": [_PL, Field, _PB, _VP, _VP, _VP, _D, _VP],
     "b200_array_op": [_I, ctypes.c_int64, Field, Field, Field, _D, _VP],
+    "b200_gather_points": [Field, _VP, ctypes.c_int64, _VP, ctypes.c_int64, _VP],
+    "b200_set_point": [Field, ctypes.c_int64, _D, _VP],
     "b200_fd_d2": [_PL, _I, _I, Field, Field, _D, _D, _D, _VP],
     "b200_laplacian": [_PL, _I, Field, Field, _D, _D, _D, _VP],
     "b200_update_pressure": [_PL, Field, Field, Field, Field, _VP],

@@ -69,6 +69,21 @@ __global__ void k_array_op(S* __restrict__ out, const S* __restrict__ a, const S
 	}
 }
 
+// Point gather (receivers) and point assignment (a source term).
+template <typename S>
+__global__ void k_gather_points(const S* __restrict__ u, const int64_t* __restrict__ idx, int64_t n,
+		S* __restrict__ out, int64_t stride)
+{
+	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (i < n) out[i * stride] = u[idx[i]];
+}
+
+template <typename S>
+__global__ void k_set_point(S* __restrict__ u, int64_t idx, S v)
+{
+	u[idx] = v;
+}
+
 template <typename S>
 __global__ void __launch_bounds__(kRowThreads) k_fill_separable(S* __restrict__ u, int64_t n1,
 		int64_t n12, Box3 b, const double* __restrict__ v1, const double* __restrict__ v2,
@@ -631,6 +646,33 @@ int b200_array_op(int op, int64_t n, b200_field out, b200_field in1, b200_field 
 		default: k_array_op<S, B200_ARRAY_ADD_UPDATE><<<blocks, kRowThreads, 0, s>>>(o, a, b, n, v); break;
 		}
 		return check_launch("k_array_op");
+	});
+}
+
+int b200_gather_points(b200_field u, const int64_t* idx, int64_t n, void* out, int64_t stride,
+		void* stream)
+{
+	if (int rc = check_field(u, "u")) return rc;
+	if (n < 0 || (n > 0 && (!idx || !out)) || stride < 1)
+		return set_error(B200_ERR_ARG, "gather: n %lld, stride %lld", (long long)n, (long long)stride);
+	if (n == 0) return B200_OK;
+	return dispatch_dtype(u.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		k_gather_points<S><<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(
+				static_cast<const S*>(u.data), idx, n, static_cast<S*>(out), stride);
+		return check_launch("k_gather_points");
+	});
+}
+
+int b200_set_point(b200_field u, int64_t idx, double value, void* stream)
+{
+	if (int rc = check_field(u, "u")) return rc;
+	if (idx < 0) return set_error(B200_ERR_ARG, "point index %lld", (long long)idx);
+	return dispatch_dtype(u.dtype, [&](auto tag) {
+		using S = decltype(tag);
+		k_set_point<S><<<1, 1, 0, as_stream(stream)>>>(static_cast<S*>(u.data), idx,
+				host_store<S>(value / (double)u.scale));
+		return check_launch("k_set_point");
 	});
 }
 

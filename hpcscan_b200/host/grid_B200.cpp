@@ -203,6 +203,7 @@ Rtn_code Grid_B200::copyGridDeviceToHost(Point_type pointType) const
 
 Rtn_code Grid_B200::copyGridHostToDevice(Point_type pointType)
 {
+	if (pointType == ALL_POINTS) host_ahead = false;
 	const b200_box b = box(pointType);
 	if (!ok(b200_copy_box_h2d(&lay, sizeof(Myfloat), d_grid, grid_3d, &b, nullptr),
 				"Grid_B200::copyGridHostToDevice"))
@@ -215,21 +216,21 @@ Rtn_code Grid_B200::copyGridHostToDevice(Point_type pointType)
 
 Rtn_code Grid_B200::write(string fileName)
 {
-	if (Config::Instance()->writeGrid && copyGridDeviceToHost(ALL_POINTS) != RTN_CODE_OK)
+	if (Config::Instance()->writeGrid && !host_ahead && copyGridDeviceToHost(ALL_POINTS) != RTN_CODE_OK)
 		return RTN_CODE_KO;
 	return Grid::write(fileName);
 }
 
 Rtn_code Grid_B200::write(Point_type pointType, string fileName)
 {
-	if (Config::Instance()->writeGrid && copyGridDeviceToHost(pointType) != RTN_CODE_OK)
+	if (Config::Instance()->writeGrid && !host_ahead && copyGridDeviceToHost(pointType) != RTN_CODE_OK)
 		return RTN_CODE_KO;
 	return Grid::write(pointType, fileName);
 }
 
 Rtn_code Grid_B200::writeGlobal(Point_type pointType, string fileName, Myint n_iter)
 {
-	if (Config::Instance()->writeGrid && pointType == INNER_POINTS &&
+	if (Config::Instance()->writeGrid && pointType == INNER_POINTS && !host_ahead &&
 			copyGridDeviceToHost(INNER_POINTS) != RTN_CODE_OK)
 		return RTN_CODE_KO;
 	return Grid::writeGlobal(pointType, fileName, n_iter);
@@ -238,13 +239,17 @@ Rtn_code Grid_B200::writeGlobal(Point_type pointType, string fileName, Myint n_i
 Rtn_code Grid_B200::read(string fileName)
 {
 	if (Grid::read(fileName) != RTN_CODE_OK) return RTN_CODE_KO;
-	return copyGridHostToDevice(ALL_POINTS);
+	const Rtn_code rc = copyGridHostToDevice(ALL_POINTS);
+	host_ahead = true;
+	return rc;
 }
 
 Rtn_code Grid_B200::read(Point_type pointType, string fileName)
 {
 	if (Grid::read(pointType, fileName) != RTN_CODE_OK) return RTN_CODE_KO;
-	return copyGridHostToDevice(pointType);
+	const Rtn_code rc = copyGridHostToDevice(pointType);
+	host_ahead = true;
+	return rc;
 }
 
 //-------------------------------------------------------------------------------------------------------
@@ -253,6 +258,7 @@ Rtn_code Grid_B200::read(Point_type pointType, string fileName)
 void Grid_B200::fill(Point_type pointType, Myfloat val)
 {
 	printDebug(MID_DEBUG, "IN Grid_B200::fill");
+	host_ahead = false;
 	const b200_box b = box(pointType);
 	if (ok(b200_fill_const(&lay, field(), &b, val, nullptr), "Grid_B200::fill"))
 		ok(b200_stream_sync(nullptr), "Grid_B200::fill");
@@ -262,6 +268,7 @@ void Grid_B200::fill(Point_type pointType, Func_type t1, Func_type t2, Func_type
 		Myfloat64 param1, Myfloat64 param2, Myfloat64 param3, Myfloat64 amp)
 {
 	printDebug(MID_DEBUG, "IN Grid_B200::fill");
+	host_ahead = false;
 	const b200_box b = box(pointType);
 	// the tables in the reference's order (axis 1, 2, 3), so that FUNC_RANDOM draws alike
 	const std::vector<Myfloat64> v1 = fill_table(b.i1s, b.i1e, dim >= DIM1, t1, Orig1, d1, param1);
@@ -274,6 +281,7 @@ void Grid_B200::fill(Point_type pointType, Func_type t1, Func_type t2, Func_type
 
 void Grid_B200::fillArray(Myfloat val)
 {
+	host_ahead = false;
 	const b200_field none{nullptr, kDtype, 1.0f};
 	if (ok(b200_array_op(B200_ARRAY_FILL, npoint, field(), none, none, val, nullptr), "Grid_B200::fillArray"))
 		ok(b200_stream_sync(nullptr), "Grid_B200::fillArray");
@@ -281,6 +289,7 @@ void Grid_B200::fillArray(Myfloat val)
 
 void Grid_B200::copyArray(const Grid& gridIn)
 {
+	host_ahead = false;
 	const Grid_B200* a = peer(gridIn, "Grid_B200::copyArray");
 	if (!a) return;
 	if (ok(b200_array_op(B200_ARRAY_COPY, npoint, field(), a->field(), a->field(), 0.0, nullptr),
@@ -290,6 +299,7 @@ void Grid_B200::copyArray(const Grid& gridIn)
 
 void Grid_B200::addArray(const Grid& gridIn1, const Grid& gridIn2)
 {
+	host_ahead = false;
 	const Grid_B200* a = peer(gridIn1, "Grid_B200::addArray");
 	const Grid_B200* b = peer(gridIn2, "Grid_B200::addArray");
 	if (!a || !b) return;
@@ -300,6 +310,7 @@ void Grid_B200::addArray(const Grid& gridIn1, const Grid& gridIn2)
 
 void Grid_B200::multiplyArray(const Grid& gridIn1, const Grid& gridIn2)
 {
+	host_ahead = false;
 	const Grid_B200* a = peer(gridIn1, "Grid_B200::multiplyArray");
 	const Grid_B200* b = peer(gridIn2, "Grid_B200::multiplyArray");
 	if (!a || !b) return;
@@ -310,6 +321,7 @@ void Grid_B200::multiplyArray(const Grid& gridIn1, const Grid& gridIn2)
 
 void Grid_B200::addUpdateArray(const Grid& gridIn)
 {
+	host_ahead = false;
 	const Grid_B200* a = peer(gridIn, "Grid_B200::addUpdateArray");
 	if (!a) return;
 	if (ok(b200_array_op(B200_ARRAY_ADD_UPDATE, npoint, field(), a->field(), a->field(), 0.0, nullptr),
@@ -449,6 +461,7 @@ Rtn_code Grid_B200::applyBoundaryCondition(BoundCond_type boundCondType)
 	int mask = 0;
 	for (int f = 0; f < 6; f++)
 		if (f / 2 < dim && getNeighbourProc(faces[f]) == MPI_PROC_NULL) mask |= 1 << f;
+	host_ahead = false;
 	if (!ok(b200_apply_boundary(&lay, field(), B200_BOUND_COND_ANTI_MIRROR, mask, nullptr),
 				"Grid_B200::applyBoundaryCondition"))
 		return RTN_CODE_KO;
@@ -471,6 +484,7 @@ Rtn_code fd_call(const Grid_B200& u, const Grid& Wgrid, Myint fdOrder, int axis,
 		error(string("IN Grid_B200::") + name + ", the other grid is not a B200 grid");
 		return RTN_CODE_KO;
 	}
+	w->markDeviceWritten();
 	const int rc = axis == 0
 			? b200_laplacian(&lay, fdOrder, u.field(), w->field(), inv2[0], inv2[1], inv2[2], nullptr)
 			: b200_fd_d2(&lay, axis, fdOrder, u.field(), w->field(), inv2[0], inv2[1], inv2[2], nullptr);
@@ -514,6 +528,7 @@ Rtn_code Grid_B200::updatePressure(Point_type, const Grid& prcGrid, const Grid& 
 	const Grid_B200* coef = peer(coefGrid, "Grid_B200::updatePressure");
 	const Grid_B200* lapla = peer(laplaGrid, "Grid_B200::updatePressure");
 	if (!prc || !coef || !lapla) return RTN_CODE_KO;
+	host_ahead = false;
 	if (!ok(b200_update_pressure(&lay, field(), prc->field(), coef->field(), lapla->field(), nullptr),
 				"Grid_B200::updatePressure"))
 		return RTN_CODE_KO;
@@ -530,6 +545,7 @@ Rtn_code Grid_B200::computePressureWithFD(Grid& prcGridIn, Grid& coefGridIn, Myi
 	const Grid_B200* prc = peer(prcGridIn, "Grid_B200::computePressureWithFD");
 	const Grid_B200* coef = peer(coefGridIn, "Grid_B200::computePressureWithFD");
 	if (!prc || !coef) return RTN_CODE_KO;
+	host_ahead = false;
 	Myfloat64 i2[3];
 	inv2(i2);
 	if (!ok(b200_compute_pressure(&lay, fdOrder, field(), prc->field(), coef->field(), i2[0], i2[1],

@@ -77,6 +77,11 @@ public:
 	// copy one point type of the grid between host (grid_3d) and device
 	Rtn_code copyGridDeviceToHost(Point_type) const;
 	Rtn_code copyGridHostToDevice(Point_type);
+	// true from read() until the device data is written again: the host array may then hold
+	// values the device does not have yet (hpcscan's Modeling set-up transforms the velocity
+	// read from file on the host), so write() must not overwrite it from the device
+	bool hostAhead(void) const { return host_ahead; }
+	void markDeviceWritten(void) const { host_ahead = false; }
 
 protected:
 	// B200 layout: the reference's padding, then n1 rounded up to 32 bytes, so that every
@@ -86,6 +91,7 @@ protected:
 private:
 	void* d_grid = nullptr;
 	b200_layout lay{};
+	mutable bool host_ahead = false;
 	b200_box box(Point_type) const;
 	// the device field of another grid of this mode, or nullptr (message printed)
 	static const Grid_B200* peer(const Grid& g, const char* caller);

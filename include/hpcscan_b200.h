@@ -118,6 +118,13 @@ int b200_fill_separable(const b200_layout* lay, b200_field u, const b200_box* bo
 int b200_array_op(int op, int64_t n, b200_field out, b200_field in1, b200_field in2, double val,
 		void* stream);
 
+/* Receivers and sources of DataAcquisition (src/data_Acquisition.cpp:286-351):
+ * out[i * stride] = u[idx[i]] for i < n (idx and out in device memory, out in u's storage type);
+ * u[idx] = value (rounded to u's storage, divided by its scale). */
+int b200_gather_points(b200_field u, const int64_t* idx, int64_t n, void* out, int64_t stride,
+		void* stream);
+int b200_set_point(b200_field u, int64_t idx, double value, void* stream);
+
 /* ---- finite-difference operators (INNER points; `u` in, `w` out) ----------------------------
  * inv2_a = (1/d_a)^2 evaluated in the compute type by the caller (src/grid.cpp:3252-3258).
  * Grid::FD_D2_N1/N2/N3 (src/grid.cpp:3232, 3566, 3900); axis = 1, 2 or 3. */

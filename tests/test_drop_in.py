@@ -110,3 +110,31 @@ def test_grid_and_memory_cases_pass_on_b200(tmp_path, case, prec):
     got = results(run(B200_BIN[prec], args + ["-testMode", "B200"], tmp_path))
     want = results(run(REF_BIN[prec], args + ["-testMode", "Baseline"], tmp_path))
     same_results(got, want, rtol=1e-4, atol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("boundary", ["FreeSurf", "None"])
+def test_modeling_b200_traces_equal_reference(tmp_path, prec, boundary):
+    """TestCase_Modeling (velocity read from file, Ricker source one point below the top,
+    receiver plane): the B200 traces (source and receivers on the device, DataAcquisition_B200)
+    equal those of the reference CPU build."""
+    import numpy as np
+    n = (48, 40, 44)
+    t = np.float32 if prec == "fp32" else np.float64
+    rng = np.random.default_rng(7)
+    vel = (2000.0 + 400.0 * np.tanh(rng.standard_normal((n[2], n[1], n[0])))).astype(t)
+    runs = {}
+    for mode, binary in (("B200", B200_BIN[prec]), ("Baseline", REF_BIN[prec])):
+        d = tmp_path / mode
+        d.mkdir()
+        vel.tofile(d / "vp.bin")
+        args = ["-testCase", "Modeling", "-testMode", mode, "-n1", str(n[0]), "-n2", str(n[1]),
+                "-n3", str(n[2]), "-modelVpFile", "vp.bin", "-nt", "160", "-boundary", boundary,
+                "-ntry", "1"]
+        run(binary, args, d)
+        runs[mode] = np.fromfile(d / "ModelingForwardPrn.trace.bin", dtype=t)
+    got, want = runs["B200"], runs["Baseline"]
+    assert got.shape == want.shape and np.abs(want).max() > 0
+    err = np.abs(got - want).max() / np.abs(want).max()
+    assert err <= (1e-6 if prec == "fp32" else 1e-13), err
