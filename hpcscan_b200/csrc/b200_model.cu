@@ -4,7 +4,7 @@
 // slowness. The reference's propagator step (src/grid.cpp:4612-5113) with an absorbing sponge
 // and a point source; the reference has no adjoint and no batching.
 //
-// Per shot, FP32 (the damping G = g1(i1) g2(i2) g3(i3), C = (v dt)^2):
+// Per shot, FP32 (the damping G = (g1(i1) g2(i2)) g3(i3), C = (v dt)^2):
 //   forward   p[n+1] = G (2 p[n] + C Lap p[n]) - G^2 p[n-1] ; p[n+1](src) += G amp s[n]
 //             traces[n] = p[n+1](receivers)
 //   adjoint   w[k] = G (2 w[k+1] + C Lap w[k+1]) - G^2 w[k+2] ; w[k](rec) += C G (d[k] - dobs[k])
@@ -43,7 +43,7 @@ struct MShot {
 __device__ __forceinline__ float damping(const MShot& m, int64_t ii)
 {
 	const int64_t z = ii / m.n12, r = ii - z * m.n12, y = r / m.n1, x = r - y * m.n1;
-	return m.g1[x] * (m.g2[y] * m.g3[z]);
+	return (m.g1[x] * m.g2[y]) * m.g3[z];
 }
 
 // The receivers of slot `slot` of every shot into row n of its traces (the source was added by

@@ -420,6 +420,17 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	const int yl = (tid / Cfg::NTX) * VY;
 	const int X = tile_x0 + xl;
 	const int Y0 = tile_y0 + yl;
+	// MODE_MODEL: g1(i1) g2(i2) of this thread's points, fixed along the march (points past the
+	// inner box are never stored: their table reads are clamped)
+	float gxy[Cfg::MODE == MODE_MODEL ? VY : 1][Cfg::MODE == MODE_MODEL ? VX : 1];
+	if constexpr (Cfg::MODE == MODE_MODEL) {
+#pragma unroll
+		for (int v = 0; v < VY; v++) {
+			const float g2 = a.g2[min(Y0 + v, a.e2)];
+#pragma unroll
+			for (int e = 0; e < VX; e++) gxy[v][e] = a.g1[min(X + e, a.e1)] * g2;
+		}
+	}
 	using Q = ZQueue<S, C>;
 	constexpr int VQ = VX / Q::W;
 	typename Q::T q[2 * RZ + 1][VY][VQ];   // values along i3 of this thread's points
@@ -655,11 +666,9 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 							} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
 								r2 = A2::add(A2::add(dx, dy), dz);
 							} else if constexpr (Cfg::MODE == MODE_MODEL) {
-								// p+ = G (2 p + C Lap p) - G^2 p-, G = g1 g2 g3 (points past the
-								// inner box are never stored: clamp their table reads)
-								const float gyz = a.g2[min(Y0 + v, a.e2)] * a.g3[k];
-								const float2 G = make_float2(a.g1[min(X + e, a.e1)] * gyz,
-										a.g1[min(X + e + 1, a.e1)] * gyz);
+								// p+ = G (2 p + C Lap p) - G^2 p-, G = (g1 g2) g3
+								const float g3 = a.g3[k];
+								const float2 G = make_float2(gxy[v][e] * g3, gxy[v][e + 1] * g3);
 								const float2 pm = make_float2(pv0[e], pv0[e + 1]);
 								const float2 cf = make_float2(pv1[e], pv1[e + 1]);
 								const float2 pc = Q::get2(yv[v + RY], e);
@@ -800,7 +809,13 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch_batch(const ZShot
 	const ZShot& sh = shots[s];
 	const int local = b - sh.cta_begin;
 	const int bx = local % sh.ntx, by = (local / sh.ntx) % sh.nty, bz = local / (sh.ntx * sh.nty);
-	zmarch_body<Cfg, true>(&sh.tm[0], &sh.tm[1], &sh.tm[2], &sh.tm[3], sh.a, bx, by, bz, slot_u,
+	// the shot's arguments in shared memory: read far more often than the tensor maps
+	__shared__ ZArgs<float> args;
+	static_assert(sizeof(ZArgs<float>) % 4 == 0, "word copy");
+	for (int i = threadIdx.x; i < (int)(sizeof(ZArgs<float>) / 4); i += blockDim.x)
+		reinterpret_cast<int*>(&args)[i] = reinterpret_cast<const int*>(&sh.a)[i];
+	__syncthreads();
+	zmarch_body<Cfg, true>(&sh.tm[0], &sh.tm[1], &sh.tm[2], &sh.tm[3], args, bx, by, bz, slot_u,
 			slot_p0, slot_out, step);
 }
 

@@ -45,7 +45,7 @@ def oracle_inputs(batch, i):
     lay = st.lay
     C = st.coef.double().cpu().numpy()
     g = [t.cpu().numpy() for t in st.sponge]
-    G = (g[0][None, None, :] * (g[1][None, :, None] * g[2][:, None, None])).astype(np.float32)
+    G = (g[0][None, None, :] * g[1][None, :, None]) * g[2][:, None, None]     # FP32, (g1 g2) g3
     G = G.reshape(-1).astype(np.float64)
     inv2 = tuple(float(np.float32(1.0 / DX) * np.float32(1.0 / DX)) for _ in range(3))
     return lay, C, G, st.src_flat, st.rec.cpu().numpy(), inv2, st.wavelet.double().cpu().numpy()
