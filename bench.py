@@ -58,9 +58,11 @@ def parse_args():
     p.add_argument("--cpu-steps", type=int, default=200,
                    help="time steps of the bounded reference CPU sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    p.add_argument("--workload", default="propa", choices=["propa", "adjoint", "modeling", "mixed"],
-                   help="propa (default, the headline), adjoint (batched checkpointed gradients) "
-                        "or modeling (batched uneven forward shots)")
+    p.add_argument("--workload", default="propa",
+                   choices=["propa", "adjoint", "modeling", "mixed", "fd"],
+                   help="propa (default, the headline), adjoint (batched checkpointed gradients), "
+                        "modeling (batched uneven forward shots), mixed (16-bit wavefields) or "
+                        "fd (the FD_D1 / FD_D2 operator test cases)")
     p.add_argument("--shots", type=int, default=0, help="shots (adjoint: 16, modeling: 64)")
     p.add_argument("--nt", type=int, default=0, help="time steps (adjoint: 2000, modeling: 1500)")
     p.add_argument("--checkpoint", type=int, default=45, help="adjoint checkpoint interval")
@@ -721,6 +723,93 @@ def mixed_arm(a):
     print(json.dumps(line))
 
 
+def run_reference_fd(case: str, n: int, order: int, threads: int):
+    """The reference's FD_D1 / FD_D2 test case (CacheBlk, its optimised CPU path) at n^3:
+    its own 'Best Gpoint/s in FD' per operator, in the order the test case runs them."""
+    from oracle import oracle
+    exe = oracle.ref_binary("f32")
+    args = [exe, "-testCase", case, "-testMode", "CacheBlk", "-fdOrder", str(order),
+            "-n1", str(n), "-n2", str(n), "-n3", str(n), "-ntry", "3"]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+    with tempfile.TemporaryDirectory() as d:
+        out = subprocess.run(args, cwd=d, capture_output=True, text=True, env=env, timeout=900)
+    if out.returncode != 0:
+        raise RuntimeError(out.stdout[-2000:] + out.stderr[-2000:])
+    return [float(x) for x in re.findall(r"Best Gpoint/s in FD\s+(\S+)", out.stdout)]
+
+
+def fd_arm(a):
+    """The single-operator test cases at n^3 (default 512), O8 (or --order), FP32:
+    FD_D1_N1/N2/N3 (src/testCase_FD_D1.cpp) and FD_D2_N1/N2/N3 + FD_LAPLACIAN
+    (src/testCase_FD_D2.cpp) on the test cases' own input sin(a1 x1) sin(a2 x2) sin(a3 x3).
+    Each operator is launched --steps times back to back after --warmup launches and timed
+    with CUDA events; one launch reads u and writes w over the inner points (8 B/point
+    algorithmic; the 1 GB pair of grids is eight times L2, so nothing stays cached between
+    launches). Beside it the reference's own CacheBlk numbers of the same test cases on the
+    host cores."""
+    import numpy as np
+    import torch
+
+    from hpcscan_b200 import layout as L
+    from hpcscan_b200.grid import Grid, init_device
+
+    n, order = a.size, a.order
+    init_device(0)
+    lay = L.b200_layout(3, n, n, n, order=order, prec="f32")
+    U, W = Grid(lay), Grid(lay)
+    U.initializeGrid()
+    W.initializeGrid()
+    U.defineUnitGrid()
+    W.defineUnitGrid()
+    U.fill(L.ALL_POINTS, L.FUNC_SINE, L.FUNC_SINE, L.FUNC_SINE, L.PI * 0.8, L.PI * 0.9, L.PI * 1.0,
+           1.1)
+    ops = ["FD_D1_N1", "FD_D1_N2", "FD_D1_N3", "FD_D2_N1", "FD_D2_N2", "FD_D2_N3", "FD_LAPLACIAN"]
+    peak, peak_src = measured_peak()
+    pts = lay.inner_points
+    res = {}
+    with ClockSampler(0) as clk:
+        clk.begin()
+        for op in ops:
+            fn = getattr(U, op)
+            for _ in range(max(a.warmup, 3)):
+                fn(L.INNER_POINTS, W, order)
+            sec = _timed(lambda: fn(L.INNER_POINTS, W, order), reps=a.steps)
+            res[op] = {"gpoint_s": round(pts / sec / 1e9, 2), "us_per_launch": round(sec * 1e6, 2),
+                       "alg_gb_s": round(8 * pts / sec / 1e9, 1),
+                       "frac_of_peak": round(8 * pts / sec / 1e9 / peak, 4)}
+        clk.end()
+    cpu = {}
+    if not a.no_cpu:
+        threads = os.cpu_count() or 1
+        try:
+            d1 = run_reference_fd("FD_D1", n, order, threads)
+            d2 = run_reference_fd("FD_D2", n, order, threads)
+            for op, v in zip(ops, d1 + d2):
+                cpu[op] = v
+            cpu["cores"] = threads
+        except Exception as e:
+            cpu = {"unavailable": str(e)[:200]}
+    d1_sec = sum(pts / (res[op]["gpoint_s"] * 1e9) for op in ops[:3])
+    value = 3 * pts / d1_sec / 1e9
+    line = {
+        "metric": f"FD_D1 GPoint/s (staggered first derivative, O{order} FP32 {n}^3, mean of the "
+                  "three axes)",
+        "value": round(value, 2), "unit": "GPoint/s", "n_gpus": 1, "steps": a.steps,
+        "warmup": max(a.warmup, 3), "ms_per_step": round(d1_sec / 3 * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (the test cases' own sine input)",
+        "config": {"workload": f"FD_D1 / FD_D2 operator test cases, O{order} FP32 {n}^3",
+                   "n": n, "order": order, "l2": "inputs 8x larger than L2, no flush"},
+        "per_operator": res,
+        "cpu_reference_gpoint_s": cpu,
+        "roofline": {"bound": "hbm", "achieved": round(8 * value, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(8 * value / peak, 4), "peak_source": peak_src,
+                     "alg_bytes": "8 B/point: read u, write w"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main():
     a = parse_args()
     if a.workload != "propa":
@@ -728,11 +817,13 @@ def main():
         if a.impl == "reference":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
-                                  "adjoint and no batched modelling path"}))
+                                  "adjoint and no batched modelling path (fd: its CacheBlk "
+                                  "numbers are in the b200 line)"}))
             return
         if world > 1 and rank != 0:
             return
-        {"adjoint": adjoint_arm, "modeling": modeling_arm, "mixed": mixed_arm}[a.workload](a)
+        {"adjoint": adjoint_arm, "modeling": modeling_arm, "mixed": mixed_arm,
+         "fd": fd_arm}[a.workload](a)
         return
     if a.impl == "reference":
         reference_arm(a)

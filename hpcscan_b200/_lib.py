@@ -81,6 +81,7 @@ SIGNATURES = {
     "b200_gather_points": [Field, _VP, ctypes.c_int64, _VP, ctypes.c_int64, _VP],
     "b200_set_point": [Field, ctypes.c_int64, _D, _VP],
     "b200_fd_d2": [_PL, _I, _I, Field, Field, _D, _D, _D, _VP],
+    "b200_fd_d1": [_PL, _I, _I, Field, Field, _D, _D, _D, _VP],
     "b200_laplacian": [_PL, _I, Field, Field, _D, _D, _D, _VP],
     "b200_update_pressure": [_PL, Field, Field, Field, Field, _VP],
     "b200_compute_pressure": [_PL, _I, Field, Field, Field, _D, _D, _D, _VP],

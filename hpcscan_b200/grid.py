@@ -22,7 +22,7 @@ import torch
 from . import _lib
 from .fdm import check_order
 from .layout import (ALL_POINTS, INNER_POINTS, GridLayout, Sampling, default_sampling,
-                     fill_tables, inv2_spacing, unit_sampling)
+                     fill_tables, inv2_spacing, inv_spacing, unit_sampling)
 
 RTN_CODE_OK, RTN_CODE_KO = 0, -1
 TORCH_DTYPE = {"f32": torch.float32, "f64": torch.float64, "f16": torch.float16,
@@ -105,6 +105,9 @@ class Grid:
     def inv2(self):
         return inv2_spacing(self.sampling, "f64" if self.layout.prec == "f64" else "f32")
 
+    def inv(self):
+        return inv_spacing(self.sampling, "f64" if self.layout.prec == "f64" else "f32")
+
     # ---- fills -----------------------------------------------------------------------------------
     def fill(self, point_type: int, *args, stream=None) -> None:
         """fill(pointType, val) or fill(pointType, f1, f2, f3, p1, p2, p3, amp)."""
@@ -167,6 +170,27 @@ class Grid:
 
     def FD_D2_N3(self, pType: int, W: "Grid", fdOrder: int, stream=None) -> int:
         return self._fd(3, W, fdOrder, "FD_D2_N3", stream)
+
+    def _fd_d1(self, axis: int, W: "Grid", order: int, stream=None) -> int:
+        if not self.sameSize(W):
+            print_error(f"Grid::FD_D1_N{axis}, grids have not same size")
+            return RTN_CODE_KO
+        check_order(order)
+        i1, i2, i3 = self.inv()
+        lay = self.c_layout()
+        _lib.call("b200_fd_d1", ctypes.byref(lay), axis, order, self.c_field(), W.c_field(),
+                  i1, i2, i3, _stream_ptr(stream))
+        return RTN_CODE_OK
+
+    def FD_D1_N1(self, pType: int, W: "Grid", fdOrder: int, stream=None) -> int:
+        """Staggered first derivative at i1 - 1/2 (src/grid.cpp:3401)."""
+        return self._fd_d1(1, W, fdOrder, stream)
+
+    def FD_D1_N2(self, pType: int, W: "Grid", fdOrder: int, stream=None) -> int:
+        return self._fd_d1(2, W, fdOrder, stream)
+
+    def FD_D1_N3(self, pType: int, W: "Grid", fdOrder: int, stream=None) -> int:
+        return self._fd_d1(3, W, fdOrder, stream)
 
     def FD_LAPLACIAN(self, pType: int, W: "Grid", fdOrder: int, stream=None) -> int:
         return self._fd(0, W, fdOrder, "FD_LAPLACIAN", stream)

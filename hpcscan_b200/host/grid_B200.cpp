@@ -192,6 +192,18 @@ Rtn_code Grid_B200::inv2(Myfloat64 out[3]) const
 	return RTN_CODE_OK;
 }
 
+// inv_d = ONE / d in Myfloat2, the factor of the FD_D1 operators (src/grid.cpp:3414-3416);
+// 0 on the axes beyond dim.
+Rtn_code Grid_B200::inv1(Myfloat64 out[3]) const
+{
+	const Myfloat64 d[3] = {d1, d2, d3};
+	for (int a = 0; a < 3; a++) {
+		const Myfloat2 inv = ONE / d[a];
+		out[a] = a + 1 > dim ? 0.0 : Myfloat64(inv);
+	}
+	return RTN_CODE_OK;
+}
+
 Rtn_code Grid_B200::copyGridDeviceToHost(Point_type pointType) const
 {
 	const b200_box b = box(pointType);
@@ -492,6 +504,38 @@ Rtn_code fd_call(const Grid_B200& u, const Grid& Wgrid, Myint fdOrder, int axis,
 	return ok(b200_stream_sync(nullptr), name) ? RTN_CODE_OK : RTN_CODE_KO;
 }
 } // namespace
+
+// Grid::FD_D1_N1/N2/N3 (src/grid.cpp:3401, 3735, 4069): same checks and messages.
+Rtn_code Grid_B200::fd_d1(const Grid& Wgrid, Myint fdOrder, int axis, const char* name) const
+{
+	if (this->sameSize(Wgrid) != true) {
+		error(string("Grid::") + name + ", grids have not same size");
+		return RTN_CODE_KO;
+	}
+	const Grid_B200* w = peer(Wgrid, name);
+	if (!w) return RTN_CODE_KO;
+	Myfloat64 inv[3];
+	inv1(inv);
+	w->markDeviceWritten();
+	if (!ok(b200_fd_d1(&lay, axis, fdOrder, field(), w->field(), inv[0], inv[1], inv[2], nullptr), name))
+		return RTN_CODE_KO;
+	return ok(b200_stream_sync(nullptr), name) ? RTN_CODE_OK : RTN_CODE_KO;
+}
+
+Rtn_code Grid_B200::FD_D1_N1(Point_type, const Grid& Wgrid, Myint fdOrder)
+{
+	return fd_d1(Wgrid, fdOrder, 1, "FD_D1_N1");
+}
+
+Rtn_code Grid_B200::FD_D1_N2(Point_type, const Grid& Wgrid, Myint fdOrder)
+{
+	return fd_d1(Wgrid, fdOrder, 2, "FD_D1_N2");
+}
+
+Rtn_code Grid_B200::FD_D1_N3(Point_type, const Grid& Wgrid, Myint fdOrder)
+{
+	return fd_d1(Wgrid, fdOrder, 3, "FD_D1_N3");
+}
 
 Rtn_code Grid_B200::FD_D2_N1(Point_type, const Grid& Wgrid, Myint fdOrder)
 {

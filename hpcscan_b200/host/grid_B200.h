@@ -63,6 +63,9 @@ public:
 	virtual Rtn_code myExchangeAll_halos();
 	virtual Rtn_code applyBoundaryCondition(BoundCond_type boundCondType);
 
+	virtual Rtn_code FD_D1_N1(Point_type pType, const Grid& Wgrid, Myint fdOrder);
+	virtual Rtn_code FD_D1_N2(Point_type pType, const Grid& Wgrid, Myint fdOrder);
+	virtual Rtn_code FD_D1_N3(Point_type pType, const Grid& Wgrid, Myint fdOrder);
 	virtual Rtn_code FD_D2_N1(Point_type pType, const Grid& Wgrid, Myint fdOrder);
 	virtual Rtn_code FD_D2_N2(Point_type pType, const Grid& Wgrid, Myint fdOrder);
 	virtual Rtn_code FD_D2_N3(Point_type pType, const Grid& Wgrid, Myint fdOrder);
@@ -96,6 +99,8 @@ private:
 	// the device field of another grid of this mode, or nullptr (message printed)
 	static const Grid_B200* peer(const Grid& g, const char* caller);
 	Rtn_code inv2(Myfloat64 out[3]) const;
+	Rtn_code inv1(Myfloat64 out[3]) const;
+	Rtn_code fd_d1(const Grid& Wgrid, Myint fdOrder, int axis, const char* name) const;
 };
 
 } // namespace hpcscan

@@ -314,6 +314,13 @@ def fill_tables(lay: GridLayout, samp: Sampling, point_type: int, funcs, params)
                  for a in range(3))
 
 
+def inv_spacing(samp: Sampling, prec: str) -> Tuple[float, float, float]:
+    """inv_d = ONE/d in the compute type Myfloat2, the FD_D1 operators' factor
+    (src/grid.cpp:3414-3416). Axes beyond dim have d = 0 and give 0."""
+    t = np.float64 if prec == "f64" else np.float32
+    return tuple(0.0 if d == 0.0 else float(t(1.0 / d)) for d in samp.d)
+
+
 def inv2_spacing(samp: Sampling, prec: str) -> Tuple[float, float, float]:
     """inv2_d = (ONE/d)^2 evaluated in the compute type Myfloat2 (src/grid.cpp:3252-3258).
     Axes beyond dim have d = 0 and are never used."""

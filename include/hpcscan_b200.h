@@ -131,6 +131,13 @@ int b200_set_point(b200_field u, int64_t idx, double value, void* stream);
 int b200_fd_d2(const b200_layout* lay, int axis, int order, b200_field u, b200_field w,
 		double inv2_1, double inv2_2, double inv2_3, void* stream);
 
+/* Grid::FD_D1_N1/N2/N3 (src/grid.cpp:3401, 3735, 4069; stencils src/fdm.h:27-275): the
+ * staggered first derivative at i - 1/2, w = ((A1 (u[i] - u[i-1]) + ...) * inv_a on INNER
+ * points, bit-identical to the CPU path. inv_a = ONE / d_a in the compute type (src/grid.cpp:
+ * 3414-3416); axis = 1..dim; the layout halo must be at least order / 2. */
+int b200_fd_d1(const b200_layout* lay, int axis, int order, b200_field u, b200_field w,
+		double inv_1, double inv_2, double inv_3, void* stream);
+
 /* Grid::FD_LAPLACIAN (src/grid.cpp:4235-4576). */
 int b200_laplacian(const b200_layout* lay, int order, b200_field u, b200_field w,
 		double inv2_1, double inv2_2, double inv2_3, void* stream);

@@ -13,7 +13,8 @@
  * (-O3 -mavx2, no FP contraction), the elementwise kernels are bit-identical.
  *
  * Reference citations are to files of vetienne74/hpcscan:
- *   coefficients, association order  src/fdm.h:277-545
+ *   coefficients, association order  src/fdm.h:277-545 (D2), 27-275 (D1)
+ *   FD_D1_N1/N2/N3                   src/grid.cpp:3401, 3735, 4069
  *   FD_D2_N1/N2/N3                   src/grid.cpp:3232, 3566, 3900
  *   FD_LAPLACIAN                     src/grid.cpp:4235-4576
  *   updatePressure                   src/grid.cpp:4579-4609
@@ -54,6 +55,23 @@ static const double D2COEF[9][9] = {
 	{-266681./88200., 7./4., -7./24., 7./108., -7./528., 7./3300., -7./30888., 1./84084.}, /* O14 */
 	{-1077749./352800., 16./9., -14./45., 112./1485., -7./396., 112./32175., -2./3861.,
 	  16./315315., -1./411840.},                                       /* O16 */
+};
+
+/* FD_D1 staggered coefficients A1..A8 per order, src/fdm.h:34-234 (index 0 unused). */
+static const double D1COEF[9][9] = {
+	{0},
+	{0, 1.0},                                                                    /* O2  */
+	{0, 9./8., -1./24.},                                                         /* O4  */
+	{0, 75./64., -25./384., 3./640.},                                            /* O6  */
+	{0, 1225./1024., -245./3072., 49./5120., -5./7168.},                         /* O8  */
+	{0, 19845./16384., -735./8192., 567./40960., -405./229376., 35./294912.},   /* O10 */
+	{0, 160083./131072., -12705./131072., 22869./1310720., -5445./1835008.,
+	  847./2359296., -63./2883584.},                                             /* O12 */
+	{0, 1288287./1048576., -429429./4194304., 429429./20971520., -61347./14680064.,
+	  13013./18874368., -3549./46137344., 231./54525952.},                       /* O14 */
+	{0, 41409225./33554432., -3578575./33554432., 3864861./167772160.,
+	  -1254825./234881024., 325325./301989888., -61425./369098752., 7425./436207616.,
+	  -143./167772160.},                                                         /* O16 */
 };
 
 int oracle_valid_order(int order)
@@ -106,6 +124,32 @@ int oracle_fd_d2_##SUF(const oracle_layout* L, int axis, int order, const T* u, 
 			for (int64_t i1 = L->s1; i1 <= L->e1; i1++) {                                     \
 				const int64_t ii = IDX(L, i1, i2, i3) ;                                       \
 				w[ii] = d2_##SUF(u, ii, st, c, r, inv2) ;                                     \
+			}                                                                                 \
+	return 0 ;                                                                                \
+}                                                                                             \
+                                                                                              \
+/* Grid::FD_D1_N1/N2/N3 (src/grid.cpp:3401,3735,4069): staggered first derivative at    */ \
+/* i - 1/2 on INNER points, ((A1 (u - u-1) + A2 (u+1 - u-2)) + ...) * inv_d; O2 has no A1 */ \
+/* factor (src/fdm.h:37-44)                                                            */ \
+int oracle_fd_d1_##SUF(const oracle_layout* L, int axis, int order, const T* u, T* w,        \
+		T inv_1, T inv_2, T inv_3)                                                            \
+{                                                                                             \
+	if (!oracle_valid_order(order) || axis < 1 || axis > 3) return -1 ;                      \
+	const int r = order / 2 ;                                                                 \
+	T c[9] ;                                                                                  \
+	for (int k = 1; k <= r; k++) c[k] = (T) D1COEF[r][k] ;                                   \
+	const int64_t st = (axis == 1) ? 1 : (axis == 2) ? L->n1 : L->n1 * L->n2 ;              \
+	const T inv = (axis == 1) ? inv_1 : (axis == 2) ? inv_2 : inv_3 ;                        \
+	_Pragma("omp parallel for collapse(2)")                                                   \
+	for (int64_t i3 = L->s3; i3 <= L->e3; i3++)                                               \
+		for (int64_t i2 = L->s2; i2 <= L->e2; i2++)                                           \
+			for (int64_t i1 = L->s1; i1 <= L->e1; i1++) {                                     \
+				const int64_t ii = IDX(L, i1, i2, i3) ;                                       \
+				if (r == 1) { w[ii] = (u[ii] - u[ii - st]) * inv ; continue ; }               \
+				T acc = c[1] * (u[ii] - u[ii - st]) ;                                         \
+				for (int k = 2; k <= r; k++)                                                  \
+					acc = acc + c[k] * (u[ii + (k - 1) * st] - u[ii - k * st]) ;              \
+				w[ii] = acc * inv ;                                                           \
 			}                                                                                 \
 	return 0 ;                                                                                \
 }                                                                                             \

@@ -55,6 +55,8 @@ def lib():
             vp = ctypes.c_void_p
             getattr(_lib, f"oracle_fd_d2_{suf}").argtypes = [P(_Layout), ctypes.c_int, ctypes.c_int,
                                                              vp, vp, ct, ct, ct]
+            getattr(_lib, f"oracle_fd_d1_{suf}").argtypes = [P(_Layout), ctypes.c_int, ctypes.c_int,
+                                                             vp, vp, ct, ct, ct]
             getattr(_lib, f"oracle_laplacian_{suf}").argtypes = [P(_Layout), ctypes.c_int, vp, vp,
                                                                  ct, ct, ct]
             getattr(_lib, f"oracle_update_pressure_{suf}").argtypes = [P(_Layout), vp, vp, vp, vp]
@@ -176,6 +178,13 @@ def alloc(lay, value=0.0):
 def fd_d2(lay, axis, u, w, inv2):
     rc = getattr(lib(), f"oracle_fd_d2_{_suf(lay)}")(_L(lay), axis, lay.order, _p(u, lay),
                                                       _p(w, lay), *inv2)
+    assert rc == 0
+
+
+def fd_d1(lay, axis, u, w, inv):
+    """Grid::FD_D1_N<axis> (src/grid.cpp:3401, 3735, 4069); inv = (1/d1, 1/d2, 1/d3)."""
+    rc = getattr(lib(), f"oracle_fd_d1_{_suf(lay)}")(_L(lay), axis, lay.order, _p(u, lay),
+                                                      _p(w, lay), *inv)
     assert rc == 0
 
 

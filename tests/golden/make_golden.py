@@ -2,13 +2,14 @@
 
 Runs the hpcscan reference CPU binaries (oracle/_ref/hpcscan_fp32|fp64, built
 unchanged from the reference sources by oracle/Makefile) with -writeGrid on
-small cases of the two hot-path test cases, FD_D2 and Propa, reads back the
+small cases of the hot-path test cases FD_D2, FD_D1 and Propa, reads back the
 grids they write (<name>.proc0.grid.bin / .grid.info, src/grid.cpp:1245-1287;
 successive writes of one name are appended), and stores:
 
   fd_*.npz     U (full grid, reference layout) and the inner points of the W
                grid of each case (Axis1..3, Laplacian), plus the L1 errors the
                reference printed;
+  fdd1_*.npz   the same for the staggered first derivative (cases Axis1..3);
   propa_*.npz  the inner points of prn at every check step, plus nt, dt and
                the reference's errTestCase.
 
@@ -53,6 +54,15 @@ FD_F64 = {"fd3_o8_k234", "fd2_o4", "fd1_o16", "fd3_all_o4", "fd3_all_o12",
           "fd3_all_o16"}
 # the order sweep stores Axis1 and the Laplacian only (Axis2/3 are covered above)
 FD_SWEEP_CASES = ("Axis1", "Laplacian3D")
+
+# FD_D1 (src/testCase_FD_D1.cpp): name, dim, (n1, n2, n3), order, extra flags
+FDD1_CASES = [
+    ("fdd1_3d_o8", 3, (20, 22, 24), 8, ["-param1", "3", "-param2", "5", "-param3", "7"]),
+    ("fdd1_2d_o6", 2, (20, 21, 1), 6, []),
+    ("fdd1_1d_o16", 1, (30, 1, 1), 16, []),
+    ("fdd1_3d_autopad_o12", 3, (21, 20, 23), 12, ["-autoPad"]),
+] + [(f"fdd1_3d_o{o}", 3, (20, 20, 21), o, []) for o in (2, 4, 6, 10, 14, 16)]
+FDD1_F64 = {"fdd1_3d_o8", "fdd1_1d_o16", "fdd1_3d_o4", "fdd1_3d_o16"}
 
 PROPA_CASES = [
     ("propa3_o8", 3, (20, 20, 20), 8, "Ac2Standard",
@@ -120,6 +130,31 @@ def gen_fd(manifest):
                 print(fn, errs)
 
 
+def gen_fd_d1(manifest):
+    for name, dim, n, order, extra in FDD1_CASES:
+        for prec in (("f32", "f64") if name in FDD1_F64 else ("f32",)):
+            with tempfile.TemporaryDirectory() as d:
+                args = ["-testCase", "FD_D1", "-testMode", "Baseline", "-dim", str(dim),
+                        "-fdOrder", str(order), "-n1", str(n[0]), "-n2", str(n[1]),
+                        "-n3", str(n[2])] + extra
+                txt = run(prec, args, d)
+                errs = [float(x) for x in
+                        re.findall(r"Test (?:PASSED|FAILED!) / L1 err\.\s+(\S+)", txt)]
+                lay = reference_layout(dim, *n, order=order, prec=prec, **parse_pad_flags(extra))
+                U, shp = read_grids(d, "FD_D1U", prec)
+                assert shp == (lay.n1, lay.n2, lay.n3), (shp, lay)
+                cases = ["Axis1", "Axis2", "Axis3"][:dim]
+                arrs = {"U": U[0]}
+                for c in cases:
+                    W, _ = read_grids(d, f"FD_D1{c}W", prec)
+                    arrs[c] = np.ascontiguousarray(lay.inner(W[0]))
+                fn = f"{name}_{prec}.npz"
+                np.savez_compressed(os.path.join(HERE, fn), **arrs)
+                manifest[fn] = {"kind": "FD_D1", "prec": prec, "dim": dim, "n": n, "order": order,
+                                "flags": extra, "cases": cases, "l1_err": errs}
+                print(fn, errs)
+
+
 def gen_propa(manifest):
     for name, dim, n, order, propa, extra in PROPA_CASES:
         for prec in ("f32", "f64"):
@@ -147,6 +182,7 @@ def gen_propa(manifest):
 def main():
     manifest = {}
     gen_fd(manifest)
+    gen_fd_d1(manifest)
     gen_propa(manifest)
     with open(os.path.join(HERE, "manifest.json"), "w") as f:
         json.dump(manifest, f, indent=1, sort_keys=True)

@@ -57,7 +57,7 @@ GRID_ARGS = ["-n1", "40", "-n2", "40", "-n3", "40", "-ntry", "1"]
 
 # ---- CPU: the factory wrapping leaves the hpcscan CPU modes as they are ------------------------
 
-@pytest.mark.parametrize("case", ["Grid", "FD_D2", "Propa"])
+@pytest.mark.parametrize("case", ["Grid", "FD_D2", "FD_D1", "Propa"])
 def test_cpu_modes_unchanged_by_b200_registration(tmp_path, case):
     args = ["-testCase", case, "-testMode", "CacheBlk"] + GRID_ARGS
     got = run(B200_BIN["fp32"], args, tmp_path)
@@ -96,6 +96,21 @@ def test_fd_d2_b200_equals_reference(tmp_path, prec, order):
             "-param1", "4", "-param2", "6", "-param3", "8", "-param4", "1", "-ntry", "1"]
     got = results(run(B200_BIN[prec], args + ["-testMode", "B200"], tmp_path))
     want = results(run(REF_BIN[prec], args + ["-testMode", "Baseline"], tmp_path))
+    same_results(got, want, rtol=1e-5, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("order,dim", [(2, 3), (4, 3), (8, 3), (12, 3), (16, 3), (6, 2), (10, 1)])
+def test_fd_d1_b200_equals_reference(tmp_path, prec, order, dim):
+    """TestCase_FD_D1: the staggered first derivative along each axis against the analytic
+    derivative on the grid shifted by half a cell; the same L1 errors and verdicts as the
+    reference CPU build."""
+    args = ["-testCase", "FD_D1", "-dim", str(dim), "-fdOrder", str(order), "-n1", "50",
+            "-n2", "44", "-n3", "38", "-param1", "3", "-param2", "5", "-param3", "7", "-ntry", "1"]
+    got = results(run(B200_BIN[prec], args + ["-testMode", "B200"], tmp_path))
+    want = results(run(REF_BIN[prec], args + ["-testMode", "Baseline"], tmp_path))
+    assert len(got) == dim
     same_results(got, want, rtol=1e-5, atol=1e-12)
 
 

@@ -122,6 +122,68 @@ def test_fd_operators_bitexact(gpu, oracle, lay):
     assert device_status() == 0
 
 
+@pytest.mark.parametrize("lay", layouts() + [L.b200_layout(3, 45, 130, 29, order=10),
+                                     L.b200_layout(3, 33, 17, 300, order=4, prec="f64")],
+                         ids=lay_id)
+def test_fd_d1_bitexact(gpu, oracle, lay):
+    """FD_D1_N1/N2/N3 (staggered first derivative) against the oracle, bit for bit; the
+    layouts cover partial x tiles and marched chunks of every remainder."""
+    u = rand_field(lay, 2)
+    samp = L.Sampling((0.013, 0.011, 0.017), (0.0, 0.0, 0.0))
+    inv = L.inv_spacing(samp, lay.prec)
+    U = dev(lay, u, samp)
+    for axis in range(1, lay.dim + 1):
+        W = dev(lay, None, samp)
+        assert getattr(U, f"FD_D1_N{axis}")(L.INNER_POINTS, W, lay.order) == 0
+        w_ref = oracle.alloc(lay)
+        oracle.fd_d1(lay, axis, u, w_ref, inv)
+        got = W.to_numpy()
+        assert np.array_equal(bits(got), bits(w_ref)), (axis, np.abs(got - w_ref).max())
+        # the halos and the outer points stay as they were (zero)
+        outside = lay.view3(got.copy())
+        outside[lay.box_slices(L.INNER_POINTS)] = 0
+        assert not outside.any()
+
+
+def test_fd_d1_fp16_storage_matches_fp32_oracle(gpu, oracle):
+    """16-bit storage, FP32 arithmetic: the FP32 oracle on the widened inputs, rounded once to
+    FP16, gives the same bits."""
+    import dataclasses
+    lay = L.b200_layout(3, 40, 21, 26, order=8, prec="f16")
+    lay32 = dataclasses.replace(lay, prec="f32")
+    u16 = rand_field(lay32, 3).astype(np.float16)
+    samp = L.Sampling((0.5, 0.25, 0.125), (0.0, 0.0, 0.0))
+    inv = L.inv_spacing(samp, "f32")
+    U = dev(lay, u16, samp)
+    for axis in (1, 2, 3):
+        W = dev(lay, None, samp)
+        assert getattr(U, f"FD_D1_N{axis}")(L.INNER_POINTS, W, 8) == 0
+        w_ref = oracle.alloc(lay32)
+        oracle.fd_d1(lay32, axis, u16.astype(np.float32), w_ref, inv)
+        got = lay.inner(W.to_numpy()).astype(np.float16)
+        want = lay32.inner(w_ref).astype(np.float16)
+        assert np.array_equal(got.view(np.uint16), want.view(np.uint16)), axis
+
+
+def test_fd_d1_rejects_bad_arguments(gpu):
+    import ctypes
+    from hpcscan_b200 import _lib
+    lay = L.b200_layout(2, 40, 33, order=8)
+    U, W = dev(lay), dev(lay)
+    cl = _lib.Layout(*lay.c_struct_fields())
+    for axis, order in ((3, 8), (0, 8), (1, 18), (1, 7)):
+        rc = _lib.load().b200_fd_d1(ctypes.byref(cl), axis, order, U.c_field(), W.c_field(),
+                                   1.0, 1.0, 1.0, None)
+        assert rc != 0, (axis, order)
+    rc = _lib.load().b200_fd_d1(ctypes.byref(cl), 1, 8, U.c_field(), U.c_field(), 1.0, 1.0, 1.0, None)
+    assert rc != 0
+    narrow = L.b200_layout(2, 40, 33, order=4)     # halo 2 < 16 / 2
+    cn = _lib.Layout(*narrow.c_struct_fields())
+    V, X = dev(narrow), dev(narrow)
+    assert _lib.load().b200_fd_d1(ctypes.byref(cn), 1, 16, V.c_field(), X.c_field(), 1.0, 1.0,
+                                 1.0, None) != 0
+
+
 @pytest.mark.parametrize("lay", layouts(), ids=lay_id)
 def test_compute_pressure_bitexact(gpu, oracle, lay):
     prc, prn, coef = rand_field(lay, 2), rand_field(lay, 3), np.abs(rand_field(lay, 4)) * 1e-3
@@ -249,6 +311,29 @@ def test_fd_golden_on_gpu(gpu, fixture):
             getattr(U, f"FD_D2_N{case[-1]}")(L.INNER_POINTS, W, meta["order"])
         else:
             U.FD_LAPLACIAN(L.INNER_POINTS, W, meta["order"])
+        assert np.array_equal(lay.inner(W.to_numpy()), gold[case]), case
+
+
+FDD1_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "FD_D1")
+
+
+@pytest.mark.parametrize("fixture", FDD1_FIXTURES)
+def test_fd_d1_golden_on_gpu(gpu, fixture):
+    """Unchanged FD_D1 test-case inputs in the B200 layout give the reference's inner values
+    of every axis bit for bit."""
+    meta = MANIFEST[fixture]
+    gold = np.load(os.path.join(GOLDEN, fixture))
+    flags = meta["flags"]
+    lay = L.b200_layout(meta["dim"], *meta["n"], order=meta["order"], prec=meta["prec"])
+    p = [flag_value(flags, f"-param{i + 1}", (0.8, 0.9, 1.0, 1.1)[i]) for i in range(4)]
+    U = dev(lay)
+    U.defineUnitGrid()
+    U.fill(L.ALL_POINTS, L.FUNC_SINE, L.FUNC_SINE, L.FUNC_SINE, L.PI * p[0], L.PI * p[1],
+           L.PI * p[2], p[3])
+    for case in meta["cases"]:
+        W = dev(lay)
+        W.defineUnitGrid()
+        assert getattr(U, f"FD_D1_N{case[-1]}")(L.INNER_POINTS, W, meta["order"]) == 0
         assert np.array_equal(lay.inner(W.to_numpy()), gold[case]), case
 
 

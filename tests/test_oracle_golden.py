@@ -53,6 +53,7 @@ def fd_input(oracle, meta):
 
 FD_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "FD_D2")
 PROPA_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "Propa")
+FDD1_FIXTURES = sorted(k for k, v in MANIFEST.items() if v["kind"] == "FD_D1")
 
 
 @pytest.mark.parametrize("fixture", FD_FIXTURES)
@@ -103,6 +104,41 @@ def test_fd_d2_l1_error_matches_reference(oracle, fixture):
     ref = meta["l1_err"]
     assert len(errs) == len(ref)
     np.testing.assert_allclose(errs, ref, rtol=2e-5)
+
+
+@pytest.mark.parametrize("fixture", FDD1_FIXTURES)
+def test_fd_d1_matches_reference(oracle, fixture):
+    """FD_D1_N1/N2/N3 (src/testCase_FD_D1.cpp) bit for bit, with the reference's printed
+    L1 errors against the analytic derivative on the grid shifted by -d/2 along the axis
+    (src/testCase_FD_D1.cpp:120-127, 204-212, 289-297)."""
+    meta = MANIFEST[fixture]
+    gold = np.load(os.path.join(GOLDEN, fixture))
+    lay, samp, u, a, p = fd_input(oracle, meta)
+    assert np.array_equal(u, gold["U"])
+    inv = L.inv_spacing(samp, lay.prec)
+    store = np.float64 if lay.prec == "f64" else np.float32
+    errs = []
+    orig = list(samp.orig)
+    for case in meta["cases"]:
+        ax = int(case[-1])
+        w = oracle.alloc(lay)
+        oracle.fd_d1(lay, ax, u, w, inv)
+        got = lay.inner(w)
+        assert np.array_equal(got, gold[case]), (case, np.abs(got - gold[case]).max())
+        # Myfloat d = getSpaceSampling(axis); shiftOriginGrid(-d/2) takes Myfloat shifts and
+        # the earlier cases' shifts are undone by +d/2 (FP64 origins: not always exact)
+        if ax > 1:
+            orig[ax - 2] = orig[ax - 2] + float(store(float(store(samp.d[ax - 2])) / 2.0))
+        orig[ax - 1] = orig[ax - 1] + float(store(-float(store(samp.d[ax - 1])) / 2.0))
+        rsamp = L.Sampling(samp.d, tuple(orig))
+        funcs = [L.FUNC_SINE] * 3
+        funcs[ax - 1] = L.FUNC_COSINE
+        tabs = L.fill_tables(lay, rsamp, L.ALL_POINTS, funcs, a)
+        r = oracle.alloc(lay)
+        oracle.fill_sep(lay, r, lay.box(L.ALL_POINTS), tabs, a[ax - 1] * p[3])
+        err = oracle.l1_err(lay, w, r, lay.box(L.INNER_POINTS))
+        errs.append(float(np.float32(err)) if lay.prec == "f32" else err)
+    np.testing.assert_allclose(errs, meta["l1_err"], rtol=2e-5)
 
 
 @pytest.mark.parametrize("fixture", PROPA_FIXTURES)
