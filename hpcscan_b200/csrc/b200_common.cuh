@@ -238,6 +238,79 @@ __device__ __forceinline__ float2 d2_axis2(F v, float2 inv2)
 	}
 }
 
+// ---- FD_D1 coefficients (reference src/fdm.h:34-234), exact rationals; index 0 unused ---------
+struct D1Table {
+	double c[9][9];
+};
+__host__ __device__ constexpr D1Table make_d1_table()
+{
+	return D1Table{{
+		{0, 0, 0, 0, 0, 0, 0, 0, 0},
+		{0, 1.0, 0, 0, 0, 0, 0, 0, 0},
+		{0, 9. / 8., -1. / 24., 0, 0, 0, 0, 0, 0},
+		{0, 75. / 64., -25. / 384., 3. / 640., 0, 0, 0, 0, 0},
+		{0, 1225. / 1024., -245. / 3072., 49. / 5120., -5. / 7168., 0, 0, 0, 0},
+		{0, 19845. / 16384., -735. / 8192., 567. / 40960., -405. / 229376., 35. / 294912., 0, 0, 0},
+		{0, 160083. / 131072., -12705. / 131072., 22869. / 1310720., -5445. / 1835008.,
+		 847. / 2359296., -63. / 2883584., 0, 0},
+		{0, 1288287. / 1048576., -429429. / 4194304., 429429. / 20971520., -61347. / 14680064.,
+		 13013. / 18874368., -3549. / 46137344., 231. / 54525952., 0},
+		{0, 41409225. / 33554432., -3578575. / 33554432., 3864861. / 167772160.,
+		 -1254825. / 234881024., 325325. / 301989888., -61425. / 369098752., 7425. / 436207616.,
+		 -143. / 167772160.},
+	}};
+}
+
+template <typename C, int R, int K>
+__device__ __forceinline__ C d1c()
+{
+	constexpr D1Table t = make_d1_table();
+	return static_cast<C>(t.c[R][K]);
+}
+
+// Staggered first derivative at i - 1/2 from v(k) = u[i + k], k = -R..R-1, with the reference's
+// association ((A1 (v0 - v-1) + A2 (v1 - v-2)) + ...) * inv; O2 has no A1 factor
+// (src/fdm.h:37-44, 51-275).
+template <typename C, int R, bool EXACT, typename F>
+__device__ __forceinline__ C d1_axis(F v, C inv)
+{
+	using A = Arith<EXACT>;
+	if constexpr (R == 1) {
+		return A::mul(A::sub(v(0), v(-1)), inv);
+	} else {
+		C acc = A::mul(d1c<C, R, 1>(), A::sub(v(0), v(-1)));
+		acc = A::mac(acc, d1c<C, R, 2>(), A::sub(v(1), v(-2)));
+		if constexpr (R >= 3) acc = A::mac(acc, d1c<C, R, 3>(), A::sub(v(2), v(-3)));
+		if constexpr (R >= 4) acc = A::mac(acc, d1c<C, R, 4>(), A::sub(v(3), v(-4)));
+		if constexpr (R >= 5) acc = A::mac(acc, d1c<C, R, 5>(), A::sub(v(4), v(-5)));
+		if constexpr (R >= 6) acc = A::mac(acc, d1c<C, R, 6>(), A::sub(v(5), v(-6)));
+		if constexpr (R >= 7) acc = A::mac(acc, d1c<C, R, 7>(), A::sub(v(6), v(-7)));
+		if constexpr (R >= 8) acc = A::mac(acc, d1c<C, R, 8>(), A::sub(v(7), v(-8)));
+		return A::mul(acc, inv);
+	}
+}
+
+// d1_axis for a pair of points (packed FP32), same association and rounding per component.
+template <int R, bool EXACT, typename F>
+__device__ __forceinline__ float2 d1_axis2(F v, float2 inv)
+{
+	using A = Arith2<EXACT>;
+	auto cf = [](float c) { return make_float2(c, c); };
+	if constexpr (R == 1) {
+		return A::mul(A::sub(v(0), v(-1)), inv);
+	} else {
+		float2 acc = A::mul(cf(d1c<float, R, 1>()), A::sub(v(0), v(-1)));
+		acc = A::mac(acc, cf(d1c<float, R, 2>()), A::sub(v(1), v(-2)));
+		if constexpr (R >= 3) acc = A::mac(acc, cf(d1c<float, R, 3>()), A::sub(v(2), v(-3)));
+		if constexpr (R >= 4) acc = A::mac(acc, cf(d1c<float, R, 4>()), A::sub(v(3), v(-4)));
+		if constexpr (R >= 5) acc = A::mac(acc, cf(d1c<float, R, 5>()), A::sub(v(4), v(-5)));
+		if constexpr (R >= 6) acc = A::mac(acc, cf(d1c<float, R, 6>()), A::sub(v(5), v(-6)));
+		if constexpr (R >= 7) acc = A::mac(acc, cf(d1c<float, R, 7>()), A::sub(v(6), v(-7)));
+		if constexpr (R >= 8) acc = A::mac(acc, cf(d1c<float, R, 8>()), A::sub(v(7), v(-8)));
+		return A::mul(acc, inv);
+	}
+}
+
 template <bool EXACT>
 __device__ __forceinline__ float2 leapfrog2(float2 prc, float2 prn, float2 coef, float2 lap)
 {

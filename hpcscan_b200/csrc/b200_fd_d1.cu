@@ -6,68 +6,21 @@
 // separately rounded in the reference's order, so the results are bit-identical to the CPU path.
 //
 // The operator reads 2R points along one axis and writes one: HBM-bound at 2 accesses per point
-// (one read, one write) when each input plane or row is fetched from DRAM once.
+// (one read, one write) when each input plane or row is fetched from DRAM once. 3-D grids whose
+// layout meets the TMA rules (every Grid_B200 grid) take the z-marching kernel
+// (b200_zmarch.cuh, MODE_D1_AXIS1..3: TMA-staged tiles, packed FP32 pairs); the kernels below
+// take 1-D and 2-D grids, 16-bit storage and the other layouts:
 //  * axis 1: one thread per point, a warp on 32 consecutive i1; the 2R - 1 neighbours of a
 //    row segment are L1 hits of the same cache lines;
 //  * axes 2 and 3: each thread marches along the axis over a chunk of points with the last 2R
 //    values in registers, so every input line is loaded once per chunk (plus 2R - 1 halo
 //    lines per chunk, mostly L2 hits); a warp covers 32 consecutive i1, coalesced.
 #include "b200_common.cuh"
+#include "b200_stencil.cuh"
 
 namespace b200 {
 
 namespace {
-
-// FD_D1 coefficients A1..AR per half width R (reference src/fdm.h:34-234), exact rationals,
-// rounded to the compute type like the reference's `const Myfloat2`.
-struct D1Table {
-	double c[9][9];
-};
-__host__ __device__ constexpr D1Table make_d1_table()
-{
-	return D1Table{{
-		{0, 0, 0, 0, 0, 0, 0, 0, 0},
-		{0, 1.0, 0, 0, 0, 0, 0, 0, 0},
-		{0, 9. / 8., -1. / 24., 0, 0, 0, 0, 0, 0},
-		{0, 75. / 64., -25. / 384., 3. / 640., 0, 0, 0, 0, 0},
-		{0, 1225. / 1024., -245. / 3072., 49. / 5120., -5. / 7168., 0, 0, 0, 0},
-		{0, 19845. / 16384., -735. / 8192., 567. / 40960., -405. / 229376., 35. / 294912., 0, 0, 0},
-		{0, 160083. / 131072., -12705. / 131072., 22869. / 1310720., -5445. / 1835008.,
-		 847. / 2359296., -63. / 2883584., 0, 0},
-		{0, 1288287. / 1048576., -429429. / 4194304., 429429. / 20971520., -61347. / 14680064.,
-		 13013. / 18874368., -3549. / 46137344., 231. / 54525952., 0},
-		{0, 41409225. / 33554432., -3578575. / 33554432., 3864861. / 167772160.,
-		 -1254825. / 234881024., 325325. / 301989888., -61425. / 369098752., 7425. / 436207616.,
-		 -143. / 167772160.},
-	}};
-}
-
-template <typename C, int R, int K>
-__device__ __forceinline__ C d1c()
-{
-	constexpr D1Table t = make_d1_table();
-	return static_cast<C>(t.c[R][K]);
-}
-
-// Staggered derivative from v(k) = u[i + k], k = -R..R-1 (src/fdm.h:37-44 for O2, 51-275).
-template <typename C, int R, typename F>
-__device__ __forceinline__ C d1_axis(F v, C inv)
-{
-	using A = Arith<true>;
-	if constexpr (R == 1) {
-		return A::mul(A::sub(v(0), v(-1)), inv);
-	} else {
-		C acc = A::mul(d1c<C, R, 1>(), A::sub(v(0), v(-1)));
-		acc = A::mac(acc, d1c<C, R, 2>(), A::sub(v(1), v(-2)));
-		if constexpr (R >= 3) acc = A::mac(acc, d1c<C, R, 3>(), A::sub(v(2), v(-3)));
-		if constexpr (R >= 4) acc = A::mac(acc, d1c<C, R, 4>(), A::sub(v(3), v(-4)));
-		if constexpr (R >= 5) acc = A::mac(acc, d1c<C, R, 5>(), A::sub(v(4), v(-5)));
-		if constexpr (R >= 6) acc = A::mac(acc, d1c<C, R, 6>(), A::sub(v(5), v(-6)));
-		if constexpr (R >= 7) acc = A::mac(acc, d1c<C, R, 7>(), A::sub(v(6), v(-7)));
-		if constexpr (R >= 8) acc = A::mac(acc, d1c<C, R, 8>(), A::sub(v(7), v(-8)));
-		return A::mul(acc, inv);
-	}
-}
 
 template <typename C>
 struct D1Args {
@@ -93,7 +46,7 @@ __global__ void __launch_bounds__(kRowThreads) k_fd_d1_axis1(D1Args<typename Sto
 	const int64_t ii = (a.s1 + x) + (a.s2 + blockIdx.y) * a.n1 + (a.s3 + blockIdx.z) * a.n12;
 	const S* __restrict__ u = static_cast<const S*>(a.u) + ii;
 	auto v = [&](int k) -> C { return Storage<S>::load(__ldg(u + k)); };
-	static_cast<S*>(a.w)[ii] = Storage<S>::store(d1_axis<C, R>(v, a.inv));
+	static_cast<S*>(a.w)[ii] = Storage<S>::store(d1_axis<C, R, true>(v, a.inv));
 }
 
 // Axes 2 (AXIS = 2: march along i2, the other index is i3) and 3 (march along i3, the other
@@ -130,14 +83,14 @@ __global__ void __launch_bounds__(kMarchX * kMarchY) k_fd_d1_march(D1Args<typena
 #pragma unroll
 			for (int m = 0; m < 2 * R - 1; m++) q[m] = q[m + 1];
 			q[2 * R - 1] = nx[t];
-			w[(int64_t)(j + t) * pm] = Storage<S>::store(d1_axis<C, R>([&](int k) { return q[R + k]; }, a.inv));
+			w[(int64_t)(j + t) * pm] = Storage<S>::store(d1_axis<C, R, true>([&](int k) { return q[R + k]; }, a.inv));
 		}
 	}
 	for (; j < j1; j++) {
 #pragma unroll
 		for (int m = 0; m < 2 * R - 1; m++) q[m] = q[m + 1];
 		q[2 * R - 1] = ld(j + R - 1);
-		w[(int64_t)j * pm] = Storage<S>::store(d1_axis<C, R>([&](int k) { return q[R + k]; }, a.inv));
+		w[(int64_t)j * pm] = Storage<S>::store(d1_axis<C, R, true>([&](int k) { return q[R + k]; }, a.inv));
 	}
 }
 
@@ -168,6 +121,11 @@ int run_fd_d1(const b200_layout* lay, int axis, int order, const b200_field& u, 
 	if (u.dtype != w.dtype) return set_error(B200_ERR_UNSUPPORTED, "FD_D1: grids of different storage types");
 	if (u.scale != w.scale) return set_error(B200_ERR_UNSUPPORTED, "FD_D1: grids of different scales");
 	if (u.data == w.data) return set_error(B200_ERR_ARG, "FD_D1: input and output are the same array");
+	const int mode = axis == 1 ? MODE_D1_AXIS1 : axis == 2 ? MODE_D1_AXIS2 : MODE_D1_AXIS3;
+	int handled = 0;
+	if (int rc = run_zmarch(mode, lay, order, u, w, nullptr, inv_1, inv_2, inv_3, s, &handled))
+		return rc;
+	if (handled) return B200_OK;
 	return dispatch_dtype(u.dtype, [&](auto tag) {
 		using S = decltype(tag);
 		using C = typename Storage<S>::C;

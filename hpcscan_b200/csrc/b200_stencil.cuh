@@ -14,6 +14,9 @@ enum StencilMode {
 	MODE_STEP = 6,       // applyBoundaryCondition(prc) fused with computePressureWithFD
 	MODE_MODEL = 7,      // damped leapfrog of the modelling engine: p+ = G (2 p + C Lap p) - G^2 p-
 	MODE_GRAD = 8,       // gradient accumulation: g += k C w Lap p
+	MODE_D1_AXIS1 = 9,   // Grid::FD_D1_N1 (staggered first derivative; inv2_* carry 1/d)
+	MODE_D1_AXIS2 = 10,  // Grid::FD_D1_N2
+	MODE_D1_AXIS3 = 11,  // Grid::FD_D1_N3
 };
 
 // Validating front end shared by all stencil entry points.
@@ -49,11 +52,12 @@ struct ZLaunch {
 constexpr int kZShapes = 3;       // shapes of the pressure and Laplacian operators
 
 // Per-operator instantiations (b200_zmarch_pressure.cu, b200_zmarch_laplacian.cu,
-// b200_zmarch_d2.cu).
+// b200_zmarch_d2.cu, b200_zmarch_d1.cu).
 int zmarch_launch_pressure(const ZLaunch& L);
 int zmarch_launch_step(const ZLaunch& L);
 int zmarch_launch_laplacian(const ZLaunch& L);
 int zmarch_launch_d2(const ZLaunch& L);
+int zmarch_launch_d1(const ZLaunch& L);
 
 // Device address of the library's error word on the current device (b200_runtime.cu).
 int device_error_word(unsigned int** ptr);

@@ -96,6 +96,9 @@ int launch(const ZLaunch& L)
 	case MODE_STEP: return zmarch_launch_step(L);
 	case MODE_PRESSURE: return zmarch_launch_pressure(L);
 	case MODE_LAPLACIAN: return zmarch_launch_laplacian(L);
+	case MODE_D1_AXIS1:
+	case MODE_D1_AXIS2:
+	case MODE_D1_AXIS3: return zmarch_launch_d1(L);
 	default: return zmarch_launch_d2(L);
 	}
 }

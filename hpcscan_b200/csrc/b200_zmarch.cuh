@@ -222,9 +222,17 @@ struct ZCfg {
 	static constexpr int TX = TX_, TY = TY_, VY = VY_, PF = PF_;
 	static constexpr int VX = 16 / sizeof(S);
 	static constexpr bool BC = (MODE == MODE_STEP);          // anti-mirror BC fused in
-	static constexpr bool XH = (MODE == MODE_D2_AXIS1 || MODE >= MODE_LAPLACIAN);
-	static constexpr bool YH = (MODE == MODE_D2_AXIS2 || MODE >= MODE_LAPLACIAN);
-	static constexpr bool ZQ = (MODE == MODE_D2_AXIS3 || MODE >= MODE_LAPLACIAN);
+	// operators of the Laplacian (the x, y and z stencils) and the staggered first derivatives
+	static constexpr bool LAP = (MODE == MODE_LAPLACIAN || MODE == MODE_PRESSURE ||
+	                             MODE == MODE_STEP || MODE == MODE_MODEL || MODE == MODE_GRAD);
+	static constexpr bool D1 = (MODE == MODE_D1_AXIS1 || MODE == MODE_D1_AXIS2 ||
+	                            MODE == MODE_D1_AXIS3);
+	static constexpr bool XH = (MODE == MODE_D2_AXIS1 || MODE == MODE_D1_AXIS1 || LAP);
+	static constexpr bool YH = (MODE == MODE_D2_AXIS2 || MODE == MODE_D1_AXIS2 || LAP);
+	static constexpr bool ZQ = (MODE == MODE_D2_AXIS3 || MODE == MODE_D1_AXIS3 || LAP);
+	// z stencil only: a plane is needed only while it is pushed into the register queue, so its
+	// slot is released on arrival and the whole ring but one slot stays in flight
+	static constexpr bool ZONLY = ZQ && !XH && !YH && !BC;
 	static constexpr bool P = (MODE == MODE_PRESSURE || MODE == MODE_STEP || MODE == MODE_MODEL ||
 	                           MODE == MODE_GRAD);
 	// pointwise tiles of the output plane: prn + coef (pressure, model), w + C + g (gradient)
@@ -234,7 +242,8 @@ struct ZCfg {
 	static constexpr int RZ = ZQ ? R : 0;
 	static constexpr int BX = TX + 2 * R4;
 	static constexpr int BY = TY + 2 * RY;
-	static constexpr int NSU = RZ + 1 + PF;                  // input-tile ring
+	static constexpr int NSU = (ZONLY && 2 * PF + 4 > RZ + 1 + PF) ? 2 * PF + 4
+	                                                               : RZ + 1 + PF;   // input-tile ring
 	static constexpr int NSP = P ? 1 + PF : 1;               // pointwise-tile ring
 	static constexpr int U_BYTES = BX * BY * (int)sizeof(S);
 	static constexpr int U_STRIDE = round_up(U_BYTES, 128);
@@ -549,6 +558,10 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 				}
 			}
 		}
+		if constexpr (Cfg::ZONLY) {
+			__syncwarp();
+			if (lane == 0) mbar_arrive(&empty_u[s]);
+		}
 		if (j >= 2 * RZ) {
 			const int o = j - 2 * RZ;
 			const int k = z0 + o;                     // output plane
@@ -648,16 +661,29 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						for (int pp = 0; pp < VX / 2; pp++) {
 							const int e = 2 * pp;
 							float2 dx = make_float2(0.f, 0.f), dy = dx, dz = dx, r2;
-							if constexpr (Cfg::XH)
+							if constexpr (Cfg::D1) {
+								// staggered first derivative, values k = -R..R-1 around the point
+								if constexpr (Cfg::MODE == MODE_D1_AXIS1)
+									r2 = d1_axis2<R, EX>([&](int kk) {
+										return make_float2(xv[R4 + e + kk], xv[R4 + e + 1 + kk]); }, i1);
+								else if constexpr (Cfg::MODE == MODE_D1_AXIS2)
+									r2 = d1_axis2<R, EX>([&](int kk) {
+										return Q::get2(yv[v + RY + kk], e); }, i2);
+								else
+									r2 = d1_axis2<R, EX>([&](int kk) {
+										return Q::get2(q[RZ + kk][v], e); }, i3);
+							}
+							if constexpr (Cfg::XH && !Cfg::D1)
 								dx = d2_axis2<R, EX>([&](int kk) {
 									return make_float2(xv[R4 + e + kk], xv[R4 + e + 1 + kk]); }, i1);
-							if constexpr (Cfg::YH)
+							if constexpr (Cfg::YH && !Cfg::D1)
 								dy = d2_axis2<R, EX>([&](int kk) {
 									return Q::get2(yv[v + RY + kk], e); }, i2);
-							if constexpr (Cfg::ZQ)
+							if constexpr (Cfg::ZQ && !Cfg::D1)
 								dz = d2_axis2<R, EX>([&](int kk) {
 									return Q::get2(q[RZ + kk][v], e); }, i3);
-							if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
+							if constexpr (Cfg::D1) {
+							} else if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
 								r2 = dx;
 							} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
 								r2 = dy;
@@ -703,22 +729,34 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						}
 					} else {
 						C dx[VX], dy[VX], dz[VX];
-						if constexpr (Cfg::XH) {
+						if constexpr (Cfg::D1) {
+#pragma unroll
+							for (int e = 0; e < VX; e++) {
+								if constexpr (Cfg::MODE == MODE_D1_AXIS1)
+									res[e] = d1_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
+								else if constexpr (Cfg::MODE == MODE_D1_AXIS2)
+									res[e] = d1_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
+								else
+									res[e] = d1_axis<C, R, EX>([&](int kk) { return Q::get(q[RZ + kk][v], e); }, a.inv2_3);
+							}
+						}
+						if constexpr (Cfg::XH && !Cfg::D1) {
 #pragma unroll
 							for (int e = 0; e < VX; e++)
 								dx[e] = d2_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
 						}
-						if constexpr (Cfg::YH) {
+						if constexpr (Cfg::YH && !Cfg::D1) {
 #pragma unroll
 							for (int e = 0; e < VX; e++)
 								dy[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
 						}
-						if constexpr (Cfg::ZQ) {
+						if constexpr (Cfg::ZQ && !Cfg::D1) {
 #pragma unroll
 							for (int e = 0; e < VX; e++)
 								dz[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(q[RZ + kk][v], e); }, a.inv2_3);
 						}
-						if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
+						if constexpr (Cfg::D1) {
+						} else if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
 #pragma unroll
 							for (int e = 0; e < VX; e++) res[e] = dx[e];
 						} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
@@ -763,13 +801,13 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 			}
 			__syncwarp();
 			if (lane == 0) {
-				mbar_arrive(&empty_u[sc]);
+				if constexpr (!Cfg::ZONLY) mbar_arrive(&empty_u[sc]);
 				if constexpr (Cfg::P) mbar_arrive(&empty_p[rp.slot]);
 			}
 			rc.advance();
 			rp.advance();
 		}
-		if constexpr (Cfg::ZQ) {
+		if constexpr (Cfg::ZQ && !Cfg::ZONLY) {
 			if (j < RZ || j >= J - RZ) {   // planes that are never a centre plane
 				__syncwarp();
 				if (lane == 0) mbar_arrive(&empty_u[s]);
