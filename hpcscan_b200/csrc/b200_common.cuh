@@ -311,6 +311,67 @@ __device__ __forceinline__ float2 d1_axis2(F v, float2 inv)
 	}
 }
 
+// d2_axis2 along i1 for the pair of points (x(0), x(1)) of a register row, x(i) the value i
+// points to the right of the pair's first point, the pair's first point at an even register.
+// Two-wide operands must be aligned register pairs, so the sums at odd offsets (whose operands
+// straddle two pairs) are computed as two scalar additions instead of regrouping registers.
+// Same association and rounding per component as d2_axis.
+template <int R, bool EXACT, typename F>
+__device__ __forceinline__ float2 d2_axis2_row(F x, float2 inv2)
+{
+	using A = Arith2<EXACT>;
+	using S1 = Arith<EXACT>;
+	auto cf = [](float c) { return make_float2(c, c); };
+	auto sum = [&](auto kc) -> float2 {
+		constexpr int k = decltype(kc)::value;
+		if constexpr (k % 2 == 0)
+			return A::add(make_float2(x(k), x(k + 1)), make_float2(x(-k), x(1 - k)));
+		else
+			return make_float2(S1::add(x(k), x(-k)), S1::add(x(k + 1), x(1 - k)));
+	};
+	float2 acc = A::mul(cf(d2c<float, R, 0>()), make_float2(x(0), x(1)));
+	if constexpr (R == 1) {
+		const float2 t = make_float2(S1::add(acc.x, x(1)), S1::add(acc.y, x(2)));
+		return A::mul(make_float2(S1::add(t.x, x(-1)), S1::add(t.y, x(0))), inv2);
+	} else {
+		acc = A::mac(acc, cf(d2c<float, R, 1>()), sum(std::integral_constant<int, 1>{}));
+		acc = A::mac(acc, cf(d2c<float, R, 2>()), sum(std::integral_constant<int, 2>{}));
+		if constexpr (R >= 3) acc = A::mac(acc, cf(d2c<float, R, 3>()), sum(std::integral_constant<int, 3>{}));
+		if constexpr (R >= 4) acc = A::mac(acc, cf(d2c<float, R, 4>()), sum(std::integral_constant<int, 4>{}));
+		if constexpr (R >= 5) acc = A::mac(acc, cf(d2c<float, R, 5>()), sum(std::integral_constant<int, 5>{}));
+		if constexpr (R >= 6) acc = A::mac(acc, cf(d2c<float, R, 6>()), sum(std::integral_constant<int, 6>{}));
+		if constexpr (R >= 7) acc = A::mac(acc, cf(d2c<float, R, 7>()), sum(std::integral_constant<int, 7>{}));
+		if constexpr (R >= 8) acc = A::mac(acc, cf(d2c<float, R, 8>()), sum(std::integral_constant<int, 8>{}));
+		return A::mul(acc, inv2);
+	}
+}
+
+// d1_axis2 along i1 for the pair of points (x(0), x(1)) of a register row (as d2_axis2_row):
+// every difference has one operand at an odd offset, so the differences are scalar.
+template <int R, bool EXACT, typename F>
+__device__ __forceinline__ float2 d1_axis2_row(F x, float2 inv)
+{
+	using A = Arith2<EXACT>;
+	using S1 = Arith<EXACT>;
+	auto cf = [](float c) { return make_float2(c, c); };
+	auto dif = [&](int k) {   // (v(k - 1) - v(-k)) for both points
+		return make_float2(S1::sub(x(k - 1), x(-k)), S1::sub(x(k), x(1 - k)));
+	};
+	if constexpr (R == 1) {
+		return A::mul(dif(1), inv);
+	} else {
+		float2 acc = A::mul(cf(d1c<float, R, 1>()), dif(1));
+		acc = A::mac(acc, cf(d1c<float, R, 2>()), dif(2));
+		if constexpr (R >= 3) acc = A::mac(acc, cf(d1c<float, R, 3>()), dif(3));
+		if constexpr (R >= 4) acc = A::mac(acc, cf(d1c<float, R, 4>()), dif(4));
+		if constexpr (R >= 5) acc = A::mac(acc, cf(d1c<float, R, 5>()), dif(5));
+		if constexpr (R >= 6) acc = A::mac(acc, cf(d1c<float, R, 6>()), dif(6));
+		if constexpr (R >= 7) acc = A::mac(acc, cf(d1c<float, R, 7>()), dif(7));
+		if constexpr (R >= 8) acc = A::mac(acc, cf(d1c<float, R, 8>()), dif(8));
+		return A::mul(acc, inv);
+	}
+}
+
 template <bool EXACT>
 __device__ __forceinline__ float2 leapfrog2(float2 prc, float2 prn, float2 coef, float2 lap)
 {

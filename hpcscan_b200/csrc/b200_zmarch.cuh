@@ -664,8 +664,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 							if constexpr (Cfg::D1) {
 								// staggered first derivative, values k = -R..R-1 around the point
 								if constexpr (Cfg::MODE == MODE_D1_AXIS1)
-									r2 = d1_axis2<R, EX>([&](int kk) {
-										return make_float2(xv[R4 + e + kk], xv[R4 + e + 1 + kk]); }, i1);
+									r2 = d1_axis2_row<R, EX>([&](int kk) { return xv[R4 + e + kk]; }, i1);
 								else if constexpr (Cfg::MODE == MODE_D1_AXIS2)
 									r2 = d1_axis2<R, EX>([&](int kk) {
 										return Q::get2(yv[v + RY + kk], e); }, i2);
@@ -674,8 +673,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 										return Q::get2(q[RZ + kk][v], e); }, i3);
 							}
 							if constexpr (Cfg::XH && !Cfg::D1)
-								dx = d2_axis2<R, EX>([&](int kk) {
-									return make_float2(xv[R4 + e + kk], xv[R4 + e + 1 + kk]); }, i1);
+								dx = d2_axis2_row<R, EX>([&](int kk) { return xv[R4 + e + kk]; }, i1);
 							if constexpr (Cfg::YH && !Cfg::D1)
 								dy = d2_axis2<R, EX>([&](int kk) {
 									return Q::get2(yv[v + RY + kk], e); }, i2);
