@@ -31,6 +31,7 @@
 #include <cuda.h>
 
 #include <cstring>
+#include <utility>
 
 #include "b200_stencil.cuh"
 
@@ -209,9 +210,21 @@ template <> struct ZQueue<__nv_bfloat16, float> {
 
 constexpr int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
+// f(integral_constant<int, 0>) .. f(integral_constant<int, N - 1>), in order
+template <typename F, int... I>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>)
+{
+	(f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f)
+{
+	static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
 // ---- kernel configuration -----------------------------------------------------------------------
 template <typename S, int R_, int MODE_, int TX_, int TY_, int VY_, int PF_, bool EXACT_ = true,
-		int MINB_ = 0, typename SC_ = S>
+		int MINB_ = 0, typename SC_ = S, int UQ_ = 2>
 struct ZCfg {
 	using Stor = S;
 	using CoefStor = SC_;                                    // coef storage (FP32 with 16-bit waves)
@@ -240,6 +253,7 @@ struct ZCfg {
 	static constexpr int R4 = XH ? round_up(R, VX) : 0;     // x halo, whole vectors
 	static constexpr int RY = YH ? R : 0;
 	static constexpr int RZ = ZQ ? R : 0;
+	static constexpr int UQ = ZQ ? UQ_ : 1;                  // planes per pass of the z loop
 	static constexpr int BX = TX + 2 * R4;
 	static constexpr int BY = TY + 2 * RY;
 	static constexpr int NSU = (ZONLY && 2 * PF + 4 > RZ + 1 + PF) ? 2 * PF + 4
@@ -442,7 +456,8 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	}
 	using Q = ZQueue<S, C>;
 	constexpr int VQ = VX / Q::W;
-	typename Q::T q[2 * RZ + 1][VY][VQ];   // values along i3 of this thread's points
+	constexpr int UQ = Cfg::UQ;
+	typename Q::T q[2 * RZ + UQ][VY][VQ];   // values along i3 of this thread's points
 	// `alive` turns false when a bounded wait runs out: the warp then skips all work but keeps
 	// the loop's barrier sequence, so no other warp is left waiting at a named barrier.
 	bool alive = true;
@@ -522,296 +537,312 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 		}
 	}
 
-	for (int j = 0; j < J; ++j) {
-		const int s = ru.slot;
-		if (alive && !__all_sync(FULL, mbar_wait(&full_u[s], ru.phase, deadline))) alive = false;
-		if constexpr (Cfg::ZQ) {
-			if (alive) {
-#pragma unroll
-				for (int i = 0; i < 2 * RZ; i++)
-#pragma unroll
+	// The loop runs UQ planes per pass, the pushes of a pass going to q[2 RZ + u] and the
+	// queue shifted by UQ once per pass: logical q[i] of sub-step u is q[u + i].
+	for (int jb = 0; jb < J; jb += UQ) {
+	static_for<UQ>([&](auto uc) {
+		constexpr int u = decltype(uc)::value;
+		const int j = jb + u;
+		if (j >= J) return;
+			const int s = ru.slot;
+			if (alive && !__all_sync(FULL, mbar_wait(&full_u[s], ru.phase, deadline))) alive = false;
+			if constexpr (Cfg::ZQ) {
+				if (alive) {
+					const S* t = su + s * UE;
+	#pragma unroll
 					for (int v = 0; v < VY; v++)
-#pragma unroll
-						for (int e = 0; e < VQ; e++) q[i][v][e] = q[i + 1][v][e];
-				const S* t = su + s * UE;
-#pragma unroll
-				for (int v = 0; v < VY; v++)
-					Q::template push<VX>(t + (yl + v + RY) * BX + R4 + xl, q[2 * RZ][v]);
-				if constexpr (Cfg::BC) {
-					// values after the boundary condition: boundary lines and planes are zero; a
-					// z-halo plane (loaded from its mirror) is minus the mirror after the i1/i2
-					// faces zeroed their lines
-					const int plane = z0 - RZ + j;
-					const bool mir = plane < a.s3 || plane > a.e3;
-					const bool zb = plane == a.s3 || plane == a.e3;
-					if (near || mir || zb) {
-#pragma unroll
-						for (int v = 0; v < VY; v++)
-#pragma unroll
-							for (int e = 0; e < VX; e++) {
-								const bool line = (qline >> (v * VX + e)) & 1u;
-								C& val = q[2 * RZ][v][e];
-								if (mir) val = line ? -C(0) : -val;
-								else if (line || zb) val = C(0);
-							}
-					}
-				}
-			}
-		}
-		if constexpr (Cfg::ZONLY) {
-			__syncwarp();
-			if (lane == 0) mbar_arrive(&empty_u[s]);
-		}
-		if (j >= 2 * RZ) {
-			const int o = j - 2 * RZ;
-			const int k = z0 + o;                     // output plane
-			const int sc = Cfg::ZQ ? rc.slot : s;      // slot holding plane k with its halos
-			const S* t = su + sc * UE;
-			const S* pt = nullptr;     // output-plane tile (prn, or w for the gradient)
-			const SC* ct = nullptr;    // coef tile
-			const S* gt = nullptr;     // gradient tile
-			if constexpr (Cfg::P) {
-				if (alive && !__all_sync(FULL, mbar_wait(&full_p[rp.slot], rp.phase, deadline)))
-					alive = false;
-				unsigned char* slot = sp + rp.slot * Cfg::SLOT_P;
-				pt = reinterpret_cast<const S*>(slot);
-				ct = reinterpret_cast<const SC*>(slot + Cfg::PT_STRIDE);
-				gt = reinterpret_cast<const S*>(slot + Cfg::PT_STRIDE + Cfg::CT_STRIDE);
-			}
-			const bool kb = Cfg::BC && (k == a.s3 || k == a.e3);
-			if constexpr (Cfg::BC) {
-				if (near || kb) {
-					S* tw = su + sc * UE;
-					if (alive && near) {
-#pragma unroll
-						for (int m = 0; m < NP1; m++) {
-							const uint32_t pe = p1[m];
-							if (pe == NO_PATCH) continue;
-							const uint32_t src = pe & 0xFFFFu;
-							const C mv = src == NEG_ZERO ? C(0) : Storage<S>::load(tw[src]);
-							tw[pe >> 16] = Storage<S>::store(-mv);
-						}
-					}
-					named_barrier_sync(1, NC);   // every consumer warp, alive or not
-					if (alive) {
-						if (near) {
-#pragma unroll
-							for (int m = 0; m < NP2; m++)
-								if (p2[m] != NO_PATCH) tw[p2[m]] = S(0.0f);
-						}
-						if (kb) {                // boundary plane: every inner point is zero
-							const int xs = tile_x0 - R4, ys = tile_y0 - RY;
-							for (int idx = tid; idx < BX * BYc; idx += NC) {
-								const int r = idx / BX, c = idx - r * BX;
-								const int x = xs + c, y = ys + r;
-								if (x >= a.s1 && x <= a.e1 && y >= a.s2 && y <= a.e2) tw[idx] = S(0.0f);
-							}
-						}
-					}
-					named_barrier_sync(1, NC);
-				}
-			}
-			if (alive) {
-				// rows of this thread's columns, plane k: (VY + 2 RY) x VX values (near a
-				// boundary the centre rows come from the patched tile too: a thread's vector
-				// can straddle the last inner point, and its halo part needs the patch)
-				typename Q::T yv[VY + 2 * RY][VQ];
-#pragma unroll
-				for (int r = 0; r < VY + 2 * RY; r++) {
-					const int v = r - RY;
-					if (v >= 0 && v < VY && Cfg::ZQ && !(Cfg::BC && (near || kb))) {
-#pragma unroll
-						for (int e = 0; e < VQ; e++) yv[r][e] = q[RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
-					} else {
-						Q::template push<VX>(t + (yl + r) * BX + R4 + xl, yv[r]);
-					}
-				}
-#pragma unroll
-				for (int v = 0; v < VY; v++) {
-					C res[VX];
-					// x-stencil vector of row v: left halo vectors, centre, right halo vectors
-					C xv[Cfg::XH ? VX + 2 * R4 : 1];
-					if constexpr (Cfg::XH) {
-#pragma unroll
-						for (int h = 0; h < R4 / VX; h++)
-							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + xl + h * VX, &xv[h * VX]);
-#pragma unroll
-						for (int e = 0; e < VX; e++) xv[R4 + e] = Q::get(yv[v + RY], e);
-#pragma unroll
-						for (int h = 0; h < R4 / VX; h++)
-							lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl + VX + h * VX,
-									&xv[R4 + VX + h * VX]);
-					}
-					if constexpr (std::is_same_v<C, float> && VX % 2 == 0) {
-						// FP32: pairs of points with the two-wide instructions
-						using A2 = Arith2<EX>;
-						const float2 i1 = make_float2(a.inv2_1, a.inv2_1);
-						const float2 i2 = make_float2(a.inv2_2, a.inv2_2);
-						const float2 i3 = make_float2(a.inv2_3, a.inv2_3);
-						// the pointwise tiles of this row, one vector load each
-						constexpr int NV = Cfg::P ? VX : 1;
-						float pv0[NV], pv1[NV], pv2[(Cfg::MODE == MODE_GRAD) ? VX : 1];
-						if constexpr (Cfg::P) {
-							lds_vec<S, float, VX>(pt + (yl + v) * TX + xl, pv0);
-							lds_vec<SC, float, VX>(ct + (yl + v) * TX + xl, pv1);
-							if constexpr (Cfg::MODE == MODE_GRAD)
-								lds_vec<S, float, VX>(gt + (yl + v) * TX + xl, pv2);
-						}
-#pragma unroll
-						for (int pp = 0; pp < VX / 2; pp++) {
-							const int e = 2 * pp;
-							float2 dx = make_float2(0.f, 0.f), dy = dx, dz = dx, r2;
-							if constexpr (Cfg::D1) {
-								// staggered first derivative, values k = -R..R-1 around the point
-								if constexpr (Cfg::MODE == MODE_D1_AXIS1)
-									r2 = d1_axis2_row<R, EX>([&](int kk) { return xv[R4 + e + kk]; }, i1);
-								else if constexpr (Cfg::MODE == MODE_D1_AXIS2)
-									r2 = d1_axis2<R, EX>([&](int kk) {
-										return Q::get2(yv[v + RY + kk], e); }, i2);
-								else
-									r2 = d1_axis2<R, EX>([&](int kk) {
-										return Q::get2(q[RZ + kk][v], e); }, i3);
-							}
-							if constexpr (Cfg::XH && !Cfg::D1)
-								dx = d2_axis2_row<R, EX>([&](int kk) { return xv[R4 + e + kk]; }, i1);
-							if constexpr (Cfg::YH && !Cfg::D1)
-								dy = d2_axis2<R, EX>([&](int kk) {
-									return Q::get2(yv[v + RY + kk], e); }, i2);
-							if constexpr (Cfg::ZQ && !Cfg::D1)
-								dz = d2_axis2<R, EX>([&](int kk) {
-									return Q::get2(q[RZ + kk][v], e); }, i3);
-							if constexpr (Cfg::D1) {
-							} else if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
-								r2 = dx;
-							} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
-								r2 = dy;
-							} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
-								r2 = dz;
-							} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
-								r2 = A2::add(A2::add(dx, dy), dz);
-							} else if constexpr (Cfg::MODE == MODE_MODEL) {
-								// p+ = G (2 p + C Lap p) - G^2 p-, G = (g1 g2) g3
-								const float g3 = a.g3[k];
-								const float2 G = make_float2(gxy[v][e] * g3, gxy[v][e + 1] * g3);
-								const float2 pm = make_float2(pv0[e], pv0[e + 1]);
-								const float2 cf = make_float2(pv1[e], pv1[e + 1]);
-								const float2 pc = Q::get2(yv[v + RY], e);
-								const float2 lap = A2::add(A2::add(dx, dy), dz);
-								const float2 t = A2::mac(A2::add(pc, pc), cf, lap);
-								const float2 gg = A2::mul(G, G);
-								r2 = A2::mac(A2::mul(make_float2(-gg.x, -gg.y), pm), G, t);
-								if (step >= 0 && k == a.src_z && Y0 + v == a.src_y) {
-									// the point source: p+(src) += G amp wavelet[step]
-									if (X + e == a.src_x) r2.x = fmaf(G.x * a.src_amp, a.wavelet[step], r2.x);
-									if (X + e + 1 == a.src_x) r2.y = fmaf(G.y * a.src_amp, a.wavelet[step], r2.y);
+						Q::template push<VX>(t + (yl + v + RY) * BX + R4 + xl, q[u + 2 * RZ][v]);
+					if constexpr (Cfg::BC) {
+						// values after the boundary condition: boundary lines and planes are zero; a
+						// z-halo plane (loaded from its mirror) is minus the mirror after the i1/i2
+						// faces zeroed their lines
+						const int plane = z0 - RZ + j;
+						const bool mir = plane < a.s3 || plane > a.e3;
+						const bool zb = plane == a.s3 || plane == a.e3;
+						if (near || mir || zb) {
+	#pragma unroll
+							for (int v = 0; v < VY; v++)
+	#pragma unroll
+								for (int e = 0; e < VX; e++) {
+									const bool line = (qline >> (v * VX + e)) & 1u;
+									C& val = q[u + 2 * RZ][v][e];
+									if (mir) val = line ? -C(0) : -val;
+									else if (line || zb) val = C(0);
 								}
-							} else if constexpr (Cfg::MODE == MODE_GRAD) {
-								// g += k C w Lap p
-								const float2 w = make_float2(pv0[e], pv0[e + 1]);
-								const float2 cf = make_float2(pv1[e], pv1[e + 1]);
-								const float2 g0 = make_float2(pv2[e], pv2[e + 1]);
-								const float2 kw = A2::mul(A2::mul(make_float2(a.kscale, a.kscale), cf), w);
-								r2 = A2::mac(g0, kw, A2::add(A2::add(dx, dy), dz));
-							} else {
-								float pn[2] = {pv0[e], pv0[e + 1]}, cf[2] = {pv1[e], pv1[e + 1]};
-								if (a.coef_scale != 1.0f) {
-									cf[0] = cf[0] * a.coef_scale;
-									cf[1] = cf[1] * a.coef_scale;
-								}
-								r2 = leapfrog2<EX>(Q::get2(yv[v + RY], e),
-										make_float2(pn[0], pn[1]), make_float2(cf[0], cf[1]),
-										A2::add(A2::add(dx, dy), dz));
-							}
-							res[e] = r2.x;
-							res[e + 1] = r2.y;
-						}
-					} else {
-						C dx[VX], dy[VX], dz[VX];
-						if constexpr (Cfg::D1) {
-#pragma unroll
-							for (int e = 0; e < VX; e++) {
-								if constexpr (Cfg::MODE == MODE_D1_AXIS1)
-									res[e] = d1_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
-								else if constexpr (Cfg::MODE == MODE_D1_AXIS2)
-									res[e] = d1_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
-								else
-									res[e] = d1_axis<C, R, EX>([&](int kk) { return Q::get(q[RZ + kk][v], e); }, a.inv2_3);
-							}
-						}
-						if constexpr (Cfg::XH && !Cfg::D1) {
-#pragma unroll
-							for (int e = 0; e < VX; e++)
-								dx[e] = d2_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
-						}
-						if constexpr (Cfg::YH && !Cfg::D1) {
-#pragma unroll
-							for (int e = 0; e < VX; e++)
-								dy[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
-						}
-						if constexpr (Cfg::ZQ && !Cfg::D1) {
-#pragma unroll
-							for (int e = 0; e < VX; e++)
-								dz[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(q[RZ + kk][v], e); }, a.inv2_3);
-						}
-						if constexpr (Cfg::D1) {
-						} else if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
-#pragma unroll
-							for (int e = 0; e < VX; e++) res[e] = dx[e];
-						} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
-#pragma unroll
-							for (int e = 0; e < VX; e++) res[e] = dy[e];
-						} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
-#pragma unroll
-							for (int e = 0; e < VX; e++) res[e] = dz[e];
-						} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
-#pragma unroll
-							for (int e = 0; e < VX; e++) res[e] = A::add(A::add(dx[e], dy[e]), dz[e]);
-						} else {
-							C pn[VX], cf[VX];
-							lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
-							lds_vec<SC, C, VX>(ct + (yl + v) * TX + xl, cf);
-#pragma unroll
-							for (int e = 0; e < VX; e++) {
-								C c = cf[e];
-								if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
-								res[e] = leapfrog<C, EX>(Q::get(yv[v + RY], e), pn[e], c,
-										A::add(A::add(dx[e], dy[e]), dz[e]));
-							}
-						}
-					}
-					const int Y = Y0 + v;
-					if (Y <= a.e2) {
-						S* dst = static_cast<S*>(a.out) + X + (int64_t)Y * a.n1 + (int64_t)k * a.n12;
-						if constexpr (SLOTS) dst += slot_out * a.out_slot_stride;
-						if (X >= a.s1 && X + VX - 1 <= a.e1) {
-							uint4 pk;
-							S* ps = reinterpret_cast<S*>(&pk);
-#pragma unroll
-							for (int e = 0; e < VX; e++) ps[e] = Storage<S>::store(res[e]);
-							*reinterpret_cast<uint4*>(dst) = pk;
-						} else {
-#pragma unroll
-							for (int e = 0; e < VX; e++)
-								if (X + e >= a.s1 && X + e <= a.e1) dst[e] = Storage<S>::store(res[e]);
 						}
 					}
 				}
 			}
-			__syncwarp();
-			if (lane == 0) {
-				if constexpr (!Cfg::ZONLY) mbar_arrive(&empty_u[sc]);
-				if constexpr (Cfg::P) mbar_arrive(&empty_p[rp.slot]);
-			}
-			rc.advance();
-			rp.advance();
-		}
-		if constexpr (Cfg::ZQ && !Cfg::ZONLY) {
-			if (j < RZ || j >= J - RZ) {   // planes that are never a centre plane
+			if constexpr (Cfg::ZONLY) {
 				__syncwarp();
 				if (lane == 0) mbar_arrive(&empty_u[s]);
 			}
+			if (j >= 2 * RZ) {
+				const int o = j - 2 * RZ;
+				const int k = z0 + o;                     // output plane
+				const int sc = Cfg::ZQ ? rc.slot : s;      // slot holding plane k with its halos
+				const S* t = su + sc * UE;
+				const S* pt = nullptr;     // output-plane tile (prn, or w for the gradient)
+				const SC* ct = nullptr;    // coef tile
+				const S* gt = nullptr;     // gradient tile
+				if constexpr (Cfg::P) {
+					if (alive && !__all_sync(FULL, mbar_wait(&full_p[rp.slot], rp.phase, deadline)))
+						alive = false;
+					unsigned char* slot = sp + rp.slot * Cfg::SLOT_P;
+					pt = reinterpret_cast<const S*>(slot);
+					ct = reinterpret_cast<const SC*>(slot + Cfg::PT_STRIDE);
+					gt = reinterpret_cast<const S*>(slot + Cfg::PT_STRIDE + Cfg::CT_STRIDE);
+				}
+				const bool kb = Cfg::BC && (k == a.s3 || k == a.e3);
+				if constexpr (Cfg::BC) {
+					if (near || kb) {
+						S* tw = su + sc * UE;
+						if (alive && near) {
+	#pragma unroll
+							for (int m = 0; m < NP1; m++) {
+								const uint32_t pe = p1[m];
+								if (pe == NO_PATCH) continue;
+								const uint32_t src = pe & 0xFFFFu;
+								const C mv = src == NEG_ZERO ? C(0) : Storage<S>::load(tw[src]);
+								tw[pe >> 16] = Storage<S>::store(-mv);
+							}
+						}
+						named_barrier_sync(1, NC);   // every consumer warp, alive or not
+						if (alive) {
+							if (near) {
+	#pragma unroll
+								for (int m = 0; m < NP2; m++)
+									if (p2[m] != NO_PATCH) tw[p2[m]] = S(0.0f);
+							}
+							if (kb) {                // boundary plane: every inner point is zero
+								const int xs = tile_x0 - R4, ys = tile_y0 - RY;
+								for (int idx = tid; idx < BX * BYc; idx += NC) {
+									const int r = idx / BX, c = idx - r * BX;
+									const int x = xs + c, y = ys + r;
+									if (x >= a.s1 && x <= a.e1 && y >= a.s2 && y <= a.e2) tw[idx] = S(0.0f);
+								}
+							}
+						}
+						named_barrier_sync(1, NC);
+					}
+				}
+				if (alive) {
+					// rows of this thread's columns, plane k: (VY + 2 RY) x VX values (near a
+					// boundary the centre rows come from the patched tile too: a thread's vector
+					// can straddle the last inner point, and its halo part needs the patch)
+					typename Q::T yv[VY + 2 * RY][VQ];
+	#pragma unroll
+					for (int r = 0; r < VY + 2 * RY; r++) {
+						const int v = r - RY;
+						if (v >= 0 && v < VY && Cfg::ZQ && !(Cfg::BC && (near || kb))) {
+	#pragma unroll
+							for (int e = 0; e < VQ; e++) yv[r][e] = q[u + RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
+						} else {
+							Q::template push<VX>(t + (yl + r) * BX + R4 + xl, yv[r]);
+						}
+					}
+	#pragma unroll
+					for (int v = 0; v < VY; v++) {
+						C res[VX];
+						// x-stencil vector of row v: left halo vectors, centre, right halo vectors
+						C xv[Cfg::XH ? VX + 2 * R4 : 1];
+						if constexpr (Cfg::XH) {
+	#pragma unroll
+							for (int h = 0; h < R4 / VX; h++)
+								lds_vec<S, C, VX>(t + (yl + v + RY) * BX + xl + h * VX, &xv[h * VX]);
+	#pragma unroll
+							for (int e = 0; e < VX; e++) xv[R4 + e] = Q::get(yv[v + RY], e);
+	#pragma unroll
+							for (int h = 0; h < R4 / VX; h++)
+								lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl + VX + h * VX,
+										&xv[R4 + VX + h * VX]);
+						}
+						if constexpr (std::is_same_v<C, float> && VX % 2 == 0) {
+							// FP32: pairs of points with the two-wide instructions
+							using A2 = Arith2<EX>;
+							const float2 i1 = make_float2(a.inv2_1, a.inv2_1);
+							const float2 i2 = make_float2(a.inv2_2, a.inv2_2);
+							const float2 i3 = make_float2(a.inv2_3, a.inv2_3);
+							// the pointwise tiles of this row, one vector load each
+							constexpr int NV = Cfg::P ? VX : 1;
+							float pv0[NV], pv1[NV], pv2[(Cfg::MODE == MODE_GRAD) ? VX : 1];
+							if constexpr (Cfg::P) {
+								lds_vec<S, float, VX>(pt + (yl + v) * TX + xl, pv0);
+								lds_vec<SC, float, VX>(ct + (yl + v) * TX + xl, pv1);
+								if constexpr (Cfg::MODE == MODE_GRAD)
+									lds_vec<S, float, VX>(gt + (yl + v) * TX + xl, pv2);
+							}
+	#pragma unroll
+							for (int pp = 0; pp < VX / 2; pp++) {
+								const int e = 2 * pp;
+								float2 dx = make_float2(0.f, 0.f), dy = dx, dz = dx, r2;
+								if constexpr (Cfg::D1) {
+									// staggered first derivative, values k = -R..R-1 around the point
+									if constexpr (Cfg::MODE == MODE_D1_AXIS1)
+										r2 = d1_axis2_row<R, EX>([&](int kk) { return xv[R4 + e + kk]; }, i1);
+									else if constexpr (Cfg::MODE == MODE_D1_AXIS2)
+										r2 = d1_axis2<R, EX>([&](int kk) {
+											return Q::get2(yv[v + RY + kk], e); }, i2);
+									else
+										r2 = d1_axis2<R, EX>([&](int kk) {
+											return Q::get2(q[u + RZ + kk][v], e); }, i3);
+								}
+								if constexpr (Cfg::XH && !Cfg::D1)
+									dx = d2_axis2_row<R, EX>([&](int kk) { return xv[R4 + e + kk]; }, i1);
+								if constexpr (Cfg::YH && !Cfg::D1)
+									dy = d2_axis2<R, EX>([&](int kk) {
+										return Q::get2(yv[v + RY + kk], e); }, i2);
+								if constexpr (Cfg::ZQ && !Cfg::D1)
+									dz = d2_axis2<R, EX>([&](int kk) {
+										return Q::get2(q[u + RZ + kk][v], e); }, i3);
+								if constexpr (Cfg::D1) {
+								} else if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
+									r2 = dx;
+								} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
+									r2 = dy;
+								} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
+									r2 = dz;
+								} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
+									r2 = A2::add(A2::add(dx, dy), dz);
+								} else if constexpr (Cfg::MODE == MODE_MODEL) {
+									// p+ = G (2 p + C Lap p) - G^2 p-, G = (g1 g2) g3
+									const float g3 = a.g3[k];
+									const float2 G = make_float2(gxy[v][e] * g3, gxy[v][e + 1] * g3);
+									const float2 pm = make_float2(pv0[e], pv0[e + 1]);
+									const float2 cf = make_float2(pv1[e], pv1[e + 1]);
+									const float2 pc = Q::get2(yv[v + RY], e);
+									const float2 lap = A2::add(A2::add(dx, dy), dz);
+									const float2 t = A2::mac(A2::add(pc, pc), cf, lap);
+									const float2 gg = A2::mul(G, G);
+									r2 = A2::mac(A2::mul(make_float2(-gg.x, -gg.y), pm), G, t);
+									if (step >= 0 && k == a.src_z && Y0 + v == a.src_y) {
+										// the point source: p+(src) += G amp wavelet[step]
+										if (X + e == a.src_x) r2.x = fmaf(G.x * a.src_amp, a.wavelet[step], r2.x);
+										if (X + e + 1 == a.src_x) r2.y = fmaf(G.y * a.src_amp, a.wavelet[step], r2.y);
+									}
+								} else if constexpr (Cfg::MODE == MODE_GRAD) {
+									// g += k C w Lap p
+									const float2 w = make_float2(pv0[e], pv0[e + 1]);
+									const float2 cf = make_float2(pv1[e], pv1[e + 1]);
+									const float2 g0 = make_float2(pv2[e], pv2[e + 1]);
+									const float2 kw = A2::mul(A2::mul(make_float2(a.kscale, a.kscale), cf), w);
+									r2 = A2::mac(g0, kw, A2::add(A2::add(dx, dy), dz));
+								} else {
+									float pn[2] = {pv0[e], pv0[e + 1]}, cf[2] = {pv1[e], pv1[e + 1]};
+									if (a.coef_scale != 1.0f) {
+										cf[0] = cf[0] * a.coef_scale;
+										cf[1] = cf[1] * a.coef_scale;
+									}
+									r2 = leapfrog2<EX>(Q::get2(yv[v + RY], e),
+											make_float2(pn[0], pn[1]), make_float2(cf[0], cf[1]),
+											A2::add(A2::add(dx, dy), dz));
+								}
+								res[e] = r2.x;
+								res[e + 1] = r2.y;
+							}
+						} else {
+							C dx[VX], dy[VX], dz[VX];
+							if constexpr (Cfg::D1) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++) {
+									if constexpr (Cfg::MODE == MODE_D1_AXIS1)
+										res[e] = d1_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
+									else if constexpr (Cfg::MODE == MODE_D1_AXIS2)
+										res[e] = d1_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
+									else
+										res[e] = d1_axis<C, R, EX>([&](int kk) { return Q::get(q[u + RZ + kk][v], e); }, a.inv2_3);
+								}
+							}
+							if constexpr (Cfg::XH && !Cfg::D1) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++)
+									dx[e] = d2_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
+							}
+							if constexpr (Cfg::YH && !Cfg::D1) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++)
+									dy[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
+							}
+							if constexpr (Cfg::ZQ && !Cfg::D1) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++)
+									dz[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(q[u + RZ + kk][v], e); }, a.inv2_3);
+							}
+							if constexpr (Cfg::D1) {
+							} else if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++) res[e] = dx[e];
+							} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++) res[e] = dy[e];
+							} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++) res[e] = dz[e];
+							} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
+	#pragma unroll
+								for (int e = 0; e < VX; e++) res[e] = A::add(A::add(dx[e], dy[e]), dz[e]);
+							} else {
+								C pn[VX], cf[VX];
+								lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
+								lds_vec<SC, C, VX>(ct + (yl + v) * TX + xl, cf);
+	#pragma unroll
+								for (int e = 0; e < VX; e++) {
+									C c = cf[e];
+									if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
+									res[e] = leapfrog<C, EX>(Q::get(yv[v + RY], e), pn[e], c,
+											A::add(A::add(dx[e], dy[e]), dz[e]));
+								}
+							}
+						}
+						const int Y = Y0 + v;
+						if (Y <= a.e2) {
+							S* dst = static_cast<S*>(a.out) + X + (int64_t)Y * a.n1 + (int64_t)k * a.n12;
+							if constexpr (SLOTS) dst += slot_out * a.out_slot_stride;
+							if (X >= a.s1 && X + VX - 1 <= a.e1) {
+								uint4 pk;
+								S* ps = reinterpret_cast<S*>(&pk);
+	#pragma unroll
+								for (int e = 0; e < VX; e++) ps[e] = Storage<S>::store(res[e]);
+								*reinterpret_cast<uint4*>(dst) = pk;
+							} else {
+	#pragma unroll
+								for (int e = 0; e < VX; e++)
+									if (X + e >= a.s1 && X + e <= a.e1) dst[e] = Storage<S>::store(res[e]);
+							}
+						}
+					}
+				}
+				__syncwarp();
+				if (lane == 0) {
+					if constexpr (!Cfg::ZONLY) mbar_arrive(&empty_u[sc]);
+					if constexpr (Cfg::P) mbar_arrive(&empty_p[rp.slot]);
+				}
+				rc.advance();
+				rp.advance();
+			}
+			if constexpr (Cfg::ZQ && !Cfg::ZONLY) {
+				if (j < RZ || j >= J - RZ) {   // planes that are never a centre plane
+					__syncwarp();
+					if (lane == 0) mbar_arrive(&empty_u[s]);
+				}
+			}
+			ru.advance();
+	});
+		if constexpr (Cfg::ZQ && UQ > 1) {
+#pragma unroll
+			for (int i = 0; i < 2 * RZ; i++)
+#pragma unroll
+				for (int v = 0; v < VY; v++)
+#pragma unroll
+					for (int e = 0; e < VQ; e++) q[i][v][e] = q[i + UQ][v][e];
+		} else if constexpr (Cfg::ZQ) {
+#pragma unroll
+			for (int i = 0; i < 2 * RZ; i++)
+#pragma unroll
+				for (int v = 0; v < VY; v++)
+#pragma unroll
+					for (int e = 0; e < VQ; e++) q[i][v][e] = q[i + 1][v][e];
 		}
-		ru.advance();
 	}
 	if (!alive && lane == 0) atomicOr(a.err, 2u);
 }
