@@ -224,7 +224,7 @@ __device__ __forceinline__ void static_for(F&& f)
 
 // ---- kernel configuration -----------------------------------------------------------------------
 template <typename S, int R_, int MODE_, int TX_, int TY_, int VY_, int PF_, bool EXACT_ = true,
-		int MINB_ = 0, typename SC_ = S, int UQ_ = 2>
+		int MINB_ = 0, typename SC_ = S, int UQ_ = 0>
 struct ZCfg {
 	using Stor = S;
 	using CoefStor = SC_;                                    // coef storage (FP32 with 16-bit waves)
@@ -253,7 +253,10 @@ struct ZCfg {
 	static constexpr int R4 = XH ? round_up(R, VX) : 0;     // x halo, whole vectors
 	static constexpr int RY = YH ? R : 0;
 	static constexpr int RZ = ZQ ? R : 0;
-	static constexpr int UQ = ZQ ? UQ_ : 1;                  // planes per pass of the z loop
+	// planes per pass of the z loop (0: four for the operators without pointwise tiles, two for
+	// the pressure updates, whose registers are the tighter; measured at 512^3 O8 on B200)
+	static constexpr int UQ = !ZQ ? 1 : UQ_ > 0 ? UQ_ : (MODE == MODE_PRESSURE || MODE == MODE_STEP ||
+	                                                     MODE == MODE_MODEL || MODE == MODE_GRAD) ? 2 : 4;
 	static constexpr int BX = TX + 2 * R4;
 	static constexpr int BY = TY + 2 * RY;
 	static constexpr int NSU = (ZONLY && 2 * PF + 4 > RZ + 1 + PF) ? 2 * PF + 4
@@ -549,7 +552,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 			if constexpr (Cfg::ZQ) {
 				if (alive) {
 					const S* t = su + s * UE;
-	#pragma unroll
+#pragma unroll
 					for (int v = 0; v < VY; v++)
 						Q::template push<VX>(t + (yl + v + RY) * BX + R4 + xl, q[u + 2 * RZ][v]);
 					if constexpr (Cfg::BC) {
@@ -560,9 +563,9 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						const bool mir = plane < a.s3 || plane > a.e3;
 						const bool zb = plane == a.s3 || plane == a.e3;
 						if (near || mir || zb) {
-	#pragma unroll
+#pragma unroll
 							for (int v = 0; v < VY; v++)
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) {
 									const bool line = (qline >> (v * VX + e)) & 1u;
 									C& val = q[u + 2 * RZ][v][e];
@@ -585,6 +588,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 				const S* pt = nullptr;     // output-plane tile (prn, or w for the gradient)
 				const SC* ct = nullptr;    // coef tile
 				const S* gt = nullptr;     // gradient tile
+				(void)pt, (void)ct, (void)gt;
 				if constexpr (Cfg::P) {
 					if (alive && !__all_sync(FULL, mbar_wait(&full_p[rp.slot], rp.phase, deadline)))
 						alive = false;
@@ -598,7 +602,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 					if (near || kb) {
 						S* tw = su + sc * UE;
 						if (alive && near) {
-	#pragma unroll
+#pragma unroll
 							for (int m = 0; m < NP1; m++) {
 								const uint32_t pe = p1[m];
 								if (pe == NO_PATCH) continue;
@@ -610,7 +614,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						named_barrier_sync(1, NC);   // every consumer warp, alive or not
 						if (alive) {
 							if (near) {
-	#pragma unroll
+#pragma unroll
 								for (int m = 0; m < NP2; m++)
 									if (p2[m] != NO_PATCH) tw[p2[m]] = S(0.0f);
 							}
@@ -631,28 +635,29 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 					// boundary the centre rows come from the patched tile too: a thread's vector
 					// can straddle the last inner point, and its halo part needs the patch)
 					typename Q::T yv[VY + 2 * RY][VQ];
-	#pragma unroll
+#pragma unroll
 					for (int r = 0; r < VY + 2 * RY; r++) {
 						const int v = r - RY;
 						if (v >= 0 && v < VY && Cfg::ZQ && !(Cfg::BC && (near || kb))) {
-	#pragma unroll
+#pragma unroll
 							for (int e = 0; e < VQ; e++) yv[r][e] = q[u + RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
 						} else {
 							Q::template push<VX>(t + (yl + r) * BX + R4 + xl, yv[r]);
 						}
 					}
-	#pragma unroll
+#pragma unroll
 					for (int v = 0; v < VY; v++) {
 						C res[VX];
 						// x-stencil vector of row v: left halo vectors, centre, right halo vectors
 						C xv[Cfg::XH ? VX + 2 * R4 : 1];
+						(void)xv;
 						if constexpr (Cfg::XH) {
-	#pragma unroll
+#pragma unroll
 							for (int h = 0; h < R4 / VX; h++)
 								lds_vec<S, C, VX>(t + (yl + v + RY) * BX + xl + h * VX, &xv[h * VX]);
-	#pragma unroll
+#pragma unroll
 							for (int e = 0; e < VX; e++) xv[R4 + e] = Q::get(yv[v + RY], e);
-	#pragma unroll
+#pragma unroll
 							for (int h = 0; h < R4 / VX; h++)
 								lds_vec<S, C, VX>(t + (yl + v + RY) * BX + R4 + xl + VX + h * VX,
 										&xv[R4 + VX + h * VX]);
@@ -666,16 +671,18 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 							// the pointwise tiles of this row, one vector load each
 							constexpr int NV = Cfg::P ? VX : 1;
 							float pv0[NV], pv1[NV], pv2[(Cfg::MODE == MODE_GRAD) ? VX : 1];
+							(void)pv0, (void)pv1, (void)pv2;
 							if constexpr (Cfg::P) {
 								lds_vec<S, float, VX>(pt + (yl + v) * TX + xl, pv0);
 								lds_vec<SC, float, VX>(ct + (yl + v) * TX + xl, pv1);
 								if constexpr (Cfg::MODE == MODE_GRAD)
 									lds_vec<S, float, VX>(gt + (yl + v) * TX + xl, pv2);
 							}
-	#pragma unroll
+#pragma unroll
 							for (int pp = 0; pp < VX / 2; pp++) {
 								const int e = 2 * pp;
 								float2 dx = make_float2(0.f, 0.f), dy = dx, dz = dx, r2;
+								(void)dx, (void)dy, (void)dz;
 								if constexpr (Cfg::D1) {
 									// staggered first derivative, values k = -R..R-1 around the point
 									if constexpr (Cfg::MODE == MODE_D1_AXIS1)
@@ -742,8 +749,9 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 							}
 						} else {
 							C dx[VX], dy[VX], dz[VX];
+							(void)dx, (void)dy, (void)dz;
 							if constexpr (Cfg::D1) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) {
 									if constexpr (Cfg::MODE == MODE_D1_AXIS1)
 										res[e] = d1_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
@@ -754,38 +762,38 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 								}
 							}
 							if constexpr (Cfg::XH && !Cfg::D1) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++)
 									dx[e] = d2_axis<C, R, EX>([&](int kk) { return xv[R4 + e + kk]; }, a.inv2_1);
 							}
 							if constexpr (Cfg::YH && !Cfg::D1) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++)
 									dy[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(yv[v + RY + kk], e); }, a.inv2_2);
 							}
 							if constexpr (Cfg::ZQ && !Cfg::D1) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++)
 									dz[e] = d2_axis<C, R, EX>([&](int kk) { return Q::get(q[u + RZ + kk][v], e); }, a.inv2_3);
 							}
 							if constexpr (Cfg::D1) {
 							} else if constexpr (Cfg::MODE == MODE_D2_AXIS1) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) res[e] = dx[e];
 							} else if constexpr (Cfg::MODE == MODE_D2_AXIS2) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) res[e] = dy[e];
 							} else if constexpr (Cfg::MODE == MODE_D2_AXIS3) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) res[e] = dz[e];
 							} else if constexpr (Cfg::MODE == MODE_LAPLACIAN) {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) res[e] = A::add(A::add(dx[e], dy[e]), dz[e]);
 							} else {
 								C pn[VX], cf[VX];
 								lds_vec<S, C, VX>(pt + (yl + v) * TX + xl, pn);
 								lds_vec<SC, C, VX>(ct + (yl + v) * TX + xl, cf);
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) {
 									C c = cf[e];
 									if (a.coef_scale != 1.0f) c = c * (C)a.coef_scale;
@@ -801,11 +809,11 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 							if (X >= a.s1 && X + VX - 1 <= a.e1) {
 								uint4 pk;
 								S* ps = reinterpret_cast<S*>(&pk);
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++) ps[e] = Storage<S>::store(res[e]);
 								*reinterpret_cast<uint4*>(dst) = pk;
 							} else {
-	#pragma unroll
+#pragma unroll
 								for (int e = 0; e < VX; e++)
 									if (X + e >= a.s1 && X + e <= a.e1) dst[e] = Storage<S>::store(res[e]);
 							}
