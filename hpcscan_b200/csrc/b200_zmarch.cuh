@@ -276,7 +276,7 @@ struct ZCfg {
 	static constexpr int NWC = NC / 32;                      // consumer warps
 	static constexpr int NT = NC + 32;                       // + one producer warp
 	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * SLOT_P : 0) +
-	                            (2 * NSU + 2 * NSP) * 8;
+	                            (2 * NSU + NSP) * 8;
 	// CTAs per SM the launch bounds ask for (registers follow: an SM has four sub-partitions
 	// of 16K registers and spreads a CTA's warps over them). Two CTAs per SM for R <= 4 with
 	// 8-warp CTAs; wider stencils keep their longer z queue in registers at one CTA per SM.
@@ -356,8 +356,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 			smem + NSU * Cfg::U_STRIDE + (Cfg::P ? NSP * Cfg::SLOT_P : 0));
 	uint64_t* full_u = bars;
 	uint64_t* empty_u = bars + NSU;
-	uint64_t* full_p = bars + 2 * NSU;
-	uint64_t* empty_p = full_p + NSP;
+	uint64_t* empty_p = bars + 2 * NSU;      // the pointwise tiles land on full_u (see the producer)
 
 	const int tile_x0 = a.x_start + bx * TX;
 	const int tile_y0 = a.s2 + by * Cfg::TY;
@@ -371,7 +370,6 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 			mbar_init(&empty_u[s], Cfg::NWC);
 		}
 		for (int s = 0; s < NSP; s++) {
-			mbar_init(&full_p[s], 1);
 			mbar_init(&empty_p[s], Cfg::NWC);
 		}
 		fence_mbar_init();
@@ -388,7 +386,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 			prefetch_tmap(tm_p1);
 			if constexpr (NPT > 2) prefetch_tmap(tm_p2);
 		}
-		int issued_u = 0, issued_p = 0;
+		int issued_u = 0;
 		bool ok = true;
 		Ring<NSU> wu;
 		Ring<NSP> wp;
@@ -398,33 +396,33 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 				ok = false;
 				break;
 			}
+			// the pointwise tiles of output plane j - 2 RZ, which the consumers compute when
+			// input plane j arrives, land on that plane's barrier: one wait per plane
+			const bool pw = Cfg::P && j >= 2 * RZ;
+			if (pw && j - 2 * RZ >= NSP && !mbar_wait(&empty_p[wp.slot], wp.phase ^ 1u, deadline)) {
+				ok = false;
+				break;
+			}
 			int plane = z0 - RZ + j;
 			if constexpr (Cfg::BC) {
 				// z-halo planes are rebuilt from their mirror planes by the consumers
 				if (plane < a.s3) plane = 2 * a.s3 - plane;
 				else if (plane > a.e3) plane = 2 * a.e3 - plane;
 			}
-			mbar_arrive_expect_tx(&full_u[wu.slot], Cfg::U_BYTES);
-			tma_tile<SLOTS>(su + wu.slot * UE, tm_u, tile_x0 - R4, tile_y0 - RY, plane, slot_u,
-					&full_u[wu.slot]);
+			uint64_t* bar = &full_u[wu.slot];
+			mbar_arrive_expect_tx(bar, Cfg::U_BYTES + (pw ? Cfg::SLOT_TX : 0));
+			tma_tile<SLOTS>(su + wu.slot * UE, tm_u, tile_x0 - R4, tile_y0 - RY, plane, slot_u, bar);
 			issued_u = j + 1;
 			wu.advance();
 			if constexpr (Cfg::P) {
-				if (j >= 2 * RZ) {
+				if (pw) {
 					const int o = j - 2 * RZ;
-					if (o >= NSP && !mbar_wait(&empty_p[wp.slot], wp.phase ^ 1u, deadline)) {
-						ok = false;
-						break;
-					}
 					unsigned char* slot = sp + wp.slot * Cfg::SLOT_P;
-					mbar_arrive_expect_tx(&full_p[wp.slot], Cfg::SLOT_TX);
-					tma_tile<SLOTS>(slot, tm_p0, tile_x0, tile_y0, z0 + o, slot_p0, &full_p[wp.slot]);
-					tma_tile<SLOTS>(slot + Cfg::PT_STRIDE, tm_p1, tile_x0, tile_y0, z0 + o, 0,
-							&full_p[wp.slot]);
+					tma_tile<SLOTS>(slot, tm_p0, tile_x0, tile_y0, z0 + o, slot_p0, bar);
+					tma_tile<SLOTS>(slot + Cfg::PT_STRIDE, tm_p1, tile_x0, tile_y0, z0 + o, 0, bar);
 					if constexpr (NPT > 2)
 						tma_tile<SLOTS>(slot + Cfg::PT_STRIDE + Cfg::CT_STRIDE, tm_p2, tile_x0, tile_y0,
-								z0 + o, 0, &full_p[wp.slot]);
-					issued_p = o + 1;
+								z0 + o, 0, bar);
 					wp.advance();
 				}
 			}
@@ -434,8 +432,6 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 		const uint64_t drain = global_timer_ns() + a.timeout_ns;
 		for (int j = max(0, issued_u - NSU); j < issued_u; ++j)
 			mbar_wait(&full_u[j % NSU], (j / NSU) & 1, drain);
-		for (int o = max(0, issued_p - NSP); o < issued_p; ++o)
-			mbar_wait(&full_p[o % NSP], (o / NSP) & 1, drain);
 		return;
 	}
 
@@ -590,8 +586,6 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 				const S* gt = nullptr;     // gradient tile
 				(void)pt, (void)ct, (void)gt;
 				if constexpr (Cfg::P) {
-					if (alive && !__all_sync(FULL, mbar_wait(&full_p[rp.slot], rp.phase, deadline)))
-						alive = false;
 					unsigned char* slot = sp + rp.slot * Cfg::SLOT_P;
 					pt = reinterpret_cast<const S*>(slot);
 					ct = reinterpret_cast<const SC*>(slot + Cfg::PT_STRIDE);
