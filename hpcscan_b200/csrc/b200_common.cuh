@@ -104,8 +104,13 @@ template <> struct Arith<false> {
 // ---- packed FP32 pairs (sm_100 two-wide add/sub/mul/fma) --------------------------------------
 // PTX add/sub/mul/fma.rn.f32x2 round each component like the scalar .rn instruction. The
 // assembler does, however, fuse a two-wide multiply into a following two-wide add (measured on
-// sm_100a with explicit .rn and with --fmad=false), so the separately rounded arithmetic keeps
-// its products scalar (__fmul_rn) and packs only the additions: bit-identical to the scalar path.
+// sm_100a with explicit .rn and with --fmad=false), and it does the same to fma(a, b, -0) with a
+// literal -0 (measured: it is a multiply to the assembler). The separately rounded arithmetic
+// therefore forms its two-wide products as fma(a, b, z) with z = -0 read from constant memory,
+// which the assembler cannot see through: a*b + (-0) is a*b exactly (and -0 + -0 = -0 keeps the
+// sign of a zero product), so the one rounding gives the IEEE product, bit-identical to the
+// scalar path.
+static __constant__ float2 c_neg_zero2 = {-0.0f, -0.0f};
 __device__ __forceinline__ float2 f2_op_add(float2 a, float2 b)
 {
 	float2 d;
@@ -145,7 +150,7 @@ template <bool EXACT> struct Arith2;
 template <> struct Arith2<true> {
 	static __device__ __forceinline__ float2 mul(float2 a, float2 b)
 	{
-		return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+		return f2_op_fma(a, b, c_neg_zero2);
 	}
 	static __device__ __forceinline__ float2 add(float2 a, float2 b) { return f2_op_add(a, b); }
 	static __device__ __forceinline__ float2 sub(float2 a, float2 b) { return f2_op_sub(a, b); }
