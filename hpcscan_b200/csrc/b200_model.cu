@@ -72,10 +72,13 @@ __global__ void k_model_residual(const MShot* __restrict__ shots, int k, int slo
 
 constexpr int kRecThreads = 128;
 
-// Stencil passes: R and the tile shape (shape 0), FP32 with fused multiply-adds.
+// Stencil passes: R and the tile shape (the pressure update's FP32 default: shape 0 up to
+// R = 2, shape 1 beyond), FP32 with fused multiply-adds.
+template <int R>
+using ModelShape = Shape<float, R, (R <= 2 ? 0 : 1)>;
 template <int R, int MODE>
-using ModelCfg = ZCfg<float, R, MODE, Shape<float, R, 0>::TX, Shape<float, R, 0>::TY,
-		Shape<float, R, 0>::VY, Shape<float, R, 0>::PF, false, Shape<float, R, 0>::MINB>;
+using ModelCfg = ZCfg<float, R, MODE, ModelShape<R>::TX, ModelShape<R>::TY, ModelShape<R>::VY,
+		ModelShape<R>::PF, false, ModelShape<R>::MINB>;
 
 }  // namespace
 }  // namespace b200

@@ -68,16 +68,16 @@ std::map<TuneKey, Tuned> g_tuned;
 std::mutex g_tune_mutex;
 int g_arith = B200_ARITH_EXACT;
 
-// Untuned defaults: the fastest shape measured at 512^3 on B200 for each storage type and
-// half width (FP32: two-row 28x64 tiles up to R = 2, 14x64 tiles for R = 3..4, 9-warp 16x64
-// tiles beyond, where the 30-row tiles run out of registers; FP64: 14x32 tiles, 30x32 tiles for
-// R = 5..7; at R = 8 those exceed the shared memory). The z-chunk follows the grid size
-// (pick_nz_chunk).
+// Untuned defaults: the fastest shape of the pressure update measured at 512^3 on B200 for each
+// storage type and half width, interleaved runs (FP32: the two-row 28x64 tiles up to R = 2, the
+// 14x64 tiles with a four-plane prefetch for R = 3..6, the 9-warp 16x64 tiles for R = 7..8;
+// FP64: 28x32 two-row tiles up to R = 2, 14x32 tiles with the four-plane prefetch for R = 3..5,
+// 16x32 9-warp tiles beyond). The z-chunk follows the grid size (pick_nz_chunk).
 Tuned default_tuning(int dtype, int R)
 {
 	Tuned t;
-	if (dtype == B200_F64) t.shape = (R <= 4 || R == 8) ? 0 : 1;
-	else t.shape = R <= 4 ? 0 : 2;
+	if (dtype == B200_F64) t.shape = R <= 2 ? 0 : R <= 5 ? 1 : 2;
+	else t.shape = R <= 2 ? 0 : R <= 6 ? 1 : 2;
 	t.nz_chunk = 0;
 	return t;
 }
