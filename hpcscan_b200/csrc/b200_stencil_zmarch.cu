@@ -72,11 +72,14 @@ int g_arith = B200_ARITH_EXACT;
 // storage type and half width, interleaved runs (FP32: the two-row 28x64 tiles up to R = 2, the
 // 14x64 tiles with a four-plane prefetch for R = 3..6, the 9-warp 16x64 tiles for R = 7..8;
 // FP64: 28x32 two-row tiles up to R = 2, 14x32 tiles with the four-plane prefetch for R = 3..5,
-// 16x32 9-warp tiles beyond). The z-chunk follows the grid size (pick_nz_chunk).
+// 16x32 9-warp tiles beyond). 16-bit wavefields (pressure update only): 8-byte thread vectors
+// with the z queue in FP32, 14-row tiles and the four-plane prefetch up to R = 4, 28-row
+// tiles beyond (launch_16bit). The z-chunk follows the grid size (pick_nz_chunk).
 Tuned default_tuning(int dtype, int R)
 {
 	Tuned t;
 	if (dtype == B200_F64) t.shape = R <= 2 ? 0 : R <= 5 ? 1 : 2;
+	else if (dtype == B200_F16 || dtype == B200_BF16) t.shape = R <= 4 ? 1 : 2;
 	else t.shape = R <= 2 ? 0 : R <= 6 ? 1 : 2;
 	t.nz_chunk = 0;
 	return t;
@@ -220,8 +223,10 @@ int b200_get_arith_mode(int* mode)
 int b200_set_stencil_config(int dtype, int order, int op, int shape, int nz_chunk)
 {
 	if (int rc = check_order(order)) return rc;
-	if (dtype != B200_F32 && dtype != B200_F64)
-		return set_error(B200_ERR_UNSUPPORTED, "tuned kernels exist for FP32 and FP64 only");
+	if (dtype != B200_F32 && dtype != B200_F64 &&
+			!((dtype == B200_F16 || dtype == B200_BF16) && op == MODE_PRESSURE))
+		return set_error(B200_ERR_UNSUPPORTED,
+				"tuned kernels exist for FP32 and FP64, and for the 16-bit pressure update");
 	if (op < MODE_D2_AXIS1 || op > MODE_STEP) return set_error(B200_ERR_ARG, "operator %d", op);
 	if (shape < -1 || shape >= (has_shapes(op) ? kZShapes : 1))
 		return set_error(B200_ERR_ARG, "shape %d", shape);

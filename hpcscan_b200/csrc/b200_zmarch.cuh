@@ -143,20 +143,27 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* tm)
 template <typename S, typename C, int N>
 __device__ __forceinline__ void lds_vec(const S* p, C* out)
 {
-	static_assert(N * sizeof(S) % 16 == 0, "vector of 16-byte multiples");
-#pragma unroll
-	for (int b = 0; b < N * (int)sizeof(S) / 16; b++) {
-		const uint4 raw = reinterpret_cast<const uint4*>(p)[b];
+	static_assert(N * sizeof(S) % 16 == 0 || N * sizeof(S) == 8, "vector of 8 or 16-byte multiples");
+	if constexpr (N * sizeof(S) == 8) {
+		const uint2 raw = *reinterpret_cast<const uint2*>(p);
 		const S* v = reinterpret_cast<const S*>(&raw);
 #pragma unroll
-		for (int i = 0; i < 16 / (int)sizeof(S); i++)
-			out[b * (16 / sizeof(S)) + i] = Storage<S>::load(v[i]);
+		for (int i = 0; i < N; i++) out[i] = Storage<S>::load(v[i]);
+	} else {
+#pragma unroll
+		for (int b = 0; b < N * (int)sizeof(S) / 16; b++) {
+			const uint4 raw = reinterpret_cast<const uint4*>(p)[b];
+			const S* v = reinterpret_cast<const S*>(&raw);
+#pragma unroll
+			for (int i = 0; i < 16 / (int)sizeof(S); i++)
+				out[b * (16 / sizeof(S)) + i] = Storage<S>::load(v[i]);
+		}
 	}
 }
 
 // The register queue along i3: the compute type per point, or, for 16-bit storage, the stored
 // values two per register (half the registers; converted to FP32 where the stencil uses them).
-template <typename S, typename C> struct ZQueue {
+template <typename S, typename C> struct ZQueueF {
 	using T = C;
 	static constexpr int W = 1;
 	static __device__ __forceinline__ C get(const T* row, int e) { return row[e]; }
@@ -167,6 +174,7 @@ template <typename S, typename C> struct ZQueue {
 	template <int N>
 	static __device__ __forceinline__ void push(const S* p, T* row) { lds_vec<S, C, N>(p, row); }
 };
+template <typename S, typename C> struct ZQueue : ZQueueF<S, C> {};
 template <> struct ZQueue<__half, float> {
 	using T = __half2;
 	static constexpr int W = 2;
@@ -224,7 +232,7 @@ __device__ __forceinline__ void static_for(F&& f)
 
 // ---- kernel configuration -----------------------------------------------------------------------
 template <typename S, int R_, int MODE_, int TX_, int TY_, int VY_, int PF_, bool EXACT_ = true,
-		int MINB_ = 0, typename SC_ = S, int UQ_ = 0>
+		int MINB_ = 0, typename SC_ = S, int UQ_ = 0, int VXB_ = 16>
 struct ZCfg {
 	using Stor = S;
 	using CoefStor = SC_;                                    // coef storage (FP32 with 16-bit waves)
@@ -233,7 +241,12 @@ struct ZCfg {
 	static constexpr int R = R_;
 	static constexpr int MODE = MODE_;
 	static constexpr int TX = TX_, TY = TY_, VY = VY_, PF = PF_;
-	static constexpr int VX = 16 / sizeof(S);
+	static constexpr int VA = 16 / sizeof(S);                // 16 bytes: the TMA alignment unit
+	static constexpr int VX = VXB_ / (int)sizeof(S);         // points per thread and row
+	static_assert((VXB_ == 16 || VXB_ == 8) && VX >= 1, "thread vectors of 8 or 16 bytes");
+	// 16-byte vectors of 16-bit values keep the z queue packed (ZQueue); 8-byte ones keep it in
+	// the compute type (ZQueueF): each value converted once, at its push
+	static constexpr bool QPACK = VXB_ == 16;
 	static constexpr bool BC = (MODE == MODE_STEP);          // anti-mirror BC fused in
 	// operators of the Laplacian (the x, y and z stencils) and the staggered first derivatives
 	static constexpr bool LAP = (MODE == MODE_LAPLACIAN || MODE == MODE_PRESSURE ||
@@ -250,7 +263,7 @@ struct ZCfg {
 	                           MODE == MODE_GRAD);
 	// pointwise tiles of the output plane: prn + coef (pressure, model), w + C + g (gradient)
 	static constexpr int NPT = (MODE == MODE_GRAD) ? 3 : 2;
-	static constexpr int R4 = XH ? round_up(R, VX) : 0;     // x halo, whole vectors
+	static constexpr int R4 = XH ? round_up(R, VA) : 0;     // x halo, whole 16-byte vectors
 	static constexpr int RY = YH ? R : 0;
 	static constexpr int RZ = ZQ ? R : 0;
 	// planes per pass of the z loop (0: four for the operators without pointwise tiles, two for
@@ -281,7 +294,7 @@ struct ZCfg {
 	// of 16K registers and spreads a CTA's warps over them). Two CTAs per SM for R <= 4 with
 	// 8-warp CTAs; wider stencils keep their longer z queue in registers at one CTA per SM.
 	static constexpr int MINB = MINB_ > 0 ? MINB_ : ((NT <= 256 && R <= 4) ? 2 : 1);
-	static_assert(TX % VX == 0 && TY % VY == 0 && NC % 32 == 0, "tile shape");
+	static_assert(TX % VA == 0 && TY % VY == 0 && NC % 32 == 0, "tile shape");
 	static_assert((MODE != MODE_MODEL && MODE != MODE_GRAD) || std::is_same_v<S, float>,
 			"the modelling engine computes in FP32");
 	static_assert(BX <= 256 && BY <= 256, "TMA box limit");
@@ -453,7 +466,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 			for (int e = 0; e < VX; e++) gxy[v][e] = a.g1[min(X + e, a.e1)] * g2;
 		}
 	}
-	using Q = ZQueue<S, C>;
+	using Q = std::conditional_t<Cfg::QPACK, ZQueue<S, C>, ZQueueF<S, C>>;
 	constexpr int VQ = VX / Q::W;
 	constexpr int UQ = Cfg::UQ;
 	typename Q::T q[2 * RZ + UQ][VY][VQ];   // values along i3 of this thread's points
@@ -801,11 +814,12 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 							S* dst = static_cast<S*>(a.out) + X + (int64_t)Y * a.n1 + (int64_t)k * a.n12;
 							if constexpr (SLOTS) dst += slot_out * a.out_slot_stride;
 							if (X >= a.s1 && X + VX - 1 <= a.e1) {
-								uint4 pk;
+								using Vec = std::conditional_t<VX * sizeof(S) == 16, uint4, uint2>;
+								Vec pk;
 								S* ps = reinterpret_cast<S*>(&pk);
 #pragma unroll
 								for (int e = 0; e < VX; e++) ps[e] = Storage<S>::store(res[e]);
-								*reinterpret_cast<uint4*>(dst) = pk;
+								*reinterpret_cast<Vec*>(dst) = pk;
 							} else {
 #pragma unroll
 								for (int e = 0; e < VX; e++)
@@ -940,7 +954,7 @@ int launch_zmarch(const ZLaunch& L)
 	a.out = out.data;
 	a.n1 = lay->n1;
 	a.n12 = lay->n1 * lay->n2;
-	a.x_start = (int)(lay->s1 / Cfg::VX) * Cfg::VX;
+	a.x_start = (int)(lay->s1 / Cfg::VA) * Cfg::VA;
 	a.s1 = (int)lay->s1; a.e1 = (int)lay->e1;
 	a.s2 = (int)lay->s2; a.e2 = (int)lay->e2;
 	a.s3 = (int)lay->s3; a.e3 = (int)lay->e3;
@@ -990,14 +1004,25 @@ int launch_shape(const ZLaunch& L)
 }
 
 // 16-bit wavefields (FP16 or BF16, with a per-field scale) computing in FP32 with fused
-// multiply-adds: one tile shape, 8 points per thread; coef in the same 16-bit type or FP32.
+// multiply-adds; coef in the same 16-bit type or FP32. Shape 0: 16-byte thread vectors (8
+// points) with the z queue kept as packed 16-bit pairs; shapes 1 and 2: 8-byte vectors (4
+// points) with the z queue in FP32, each value converted once (14-row tiles and a four-plane
+// prefetch, or 28-row tiles).
+template <int MODE, int R, typename S, typename SC>
+int launch_16bit_coef(const ZLaunch& L)
+{
+	switch (L.shape) {
+	case 1: return launch_zmarch<ZCfg<S, R, MODE, 64, 14, 1, 4, false, 0, SC, 0, 8>>(L);
+	case 2: return launch_zmarch<ZCfg<S, R, MODE, 64, (R <= 4 ? 28 : 16), 1, 2, false, 0, SC, 0, 8>>(L);
+	default: return launch_zmarch<ZCfg<S, R, MODE, 64, (R <= 4 ? 28 : 16), 1, 2, false, 0, SC>>(L);
+	}
+}
+
 template <int MODE, int R, typename S>
 int launch_16bit(const ZLaunch& L)
 {
-	constexpr int TY = R <= 4 ? 28 : 16;
-	if (L.coef && L.coef->dtype == B200_F32)
-		return launch_zmarch<ZCfg<S, R, MODE, 64, TY, 1, 2, false, 0, float>>(L);
-	return launch_zmarch<ZCfg<S, R, MODE, 64, TY, 1, 2, false, 0, S>>(L);
+	if (L.coef && L.coef->dtype == B200_F32) return launch_16bit_coef<MODE, R, S, float>(L);
+	return launch_16bit_coef<MODE, R, S, S>(L);
 }
 
 // Dispatch storage type, half width, shape and arithmetic for one operator. NSHAPES and

@@ -431,3 +431,32 @@ def test_fused_step_small_grid_falls_back(gpu, oracle):
     oracle.compute_pressure(lay, prn, prc, coef, L.inv2_spacing(samp, lay.prec))
     assert np.array_equal(bits(Prn.to_numpy()), bits(prn))
     assert np.array_equal(bits(Prc.to_numpy()), bits(prc))
+
+
+@pytest.mark.parametrize("lay", [L.b200_layout(3, 70, 33, 41, order=10), L.b200_layout(3, 45, 30, 37, order=16),
+                                 L.b200_layout(3, 37, 20, 23, order=8), L.b200_layout(3, 41, 30, 26, order=12, prec="f64"),
+                                 L.b200_layout(3, 36, 22, 19, order=16, prec="f64")], ids=lay_id)
+@pytest.mark.parametrize("shape", [0, 1, 2])
+def test_pressure_and_laplacian_every_shape(gpu, oracle, lay, shape):
+    """computePressureWithFD and FD_LAPLACIAN through every tile shape of the z-marching kernel
+    (two- and four-plane prefetch, 8- and 9-warp tiles), bit for bit."""
+    from hpcscan_b200 import _lib
+    dt = _lib.DTYPE_CODE[lay.prec]
+    for op in (_lib.OP_PRESSURE, _lib.OP_LAPLACIAN):
+        _lib.call("b200_set_stencil_config", dt, lay.order, op, shape, 0)
+    try:
+        prc, prn, coef = rand_field(lay, 21), rand_field(lay, 22), np.abs(rand_field(lay, 23)) * 1e-3
+        samp = L.Sampling((0.02, 0.03, 0.025), (0.0, 0.0, 0.0))
+        inv2 = L.inv2_spacing(samp, lay.prec)
+        Prc, Prn, Coef, W = dev(lay, prc, samp), dev(lay, prn, samp), dev(lay, coef, samp), dev(lay, None, samp)
+        assert Prn.computePressureWithFD(Prc, Coef, lay.order) == 0
+        assert Prc.FD_LAPLACIAN(L.INNER_POINTS, W, lay.order) == 0
+        oracle.compute_pressure(lay, prn, prc, coef, inv2)
+        w = oracle.alloc(lay)
+        oracle.laplacian(lay, prc, w, inv2)
+        assert np.array_equal(bits(Prn.to_numpy()), bits(prn))
+        assert np.array_equal(bits(W.to_numpy()), bits(w))
+        assert device_status() == 0
+    finally:
+        for op in (_lib.OP_PRESSURE, _lib.OP_LAPLACIAN):
+            _lib.call("b200_set_stencil_config", dt, lay.order, op, -1, 0)
