@@ -21,6 +21,22 @@ Box3 to_box3(const b200_box* b)
 			(int)(b->i3e - b->i3s + 1)};
 }
 
+// Row index -> (i2, i3) offsets of a box; 32-bit division (boxes of fewer than 2^31 rows,
+// checked by box_rows_ok on the host).
+__device__ __forceinline__ void row_yz(int64_t row, int ny, int& y, int& z)
+{
+	const unsigned r = (unsigned)row;
+	z = (int)(r / (unsigned)ny);
+	y = (int)(r - (unsigned)z * (unsigned)ny);
+}
+
+int box_rows_ok(const Box3& b)
+{
+	if ((int64_t)b.ny * b.nz >= (1LL << 31))
+		return set_error(B200_ERR_UNSUPPORTED, "box of %d x %d rows (2^31 at most)", b.ny, b.nz);
+	return B200_OK;
+}
+
 // Row walk: the blocks of a grid take the rows (i2, i3) of a box, kUnroll rows at a time, and
 // the threads of a block stride along i1 (coalesced). A grid of at most 8 blocks per SM, each
 // thread with kUnroll independent loads in flight per step.
@@ -41,7 +57,8 @@ __global__ void __launch_bounds__(kRowThreads) k_fill_const(S* __restrict__ u, i
 {
 	const int64_t rows = (int64_t)b.ny * b.nz;
 	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
-		const int64_t y = row % b.ny, z = row / b.ny;
+		int y, z;
+		row_yz(row, b.ny, y, z);
 		S* dst = u + b.i1s + (b.i2s + y) * n1 + (b.i3s + z) * n12;
 		for (int x = threadIdx.x; x < b.nx; x += blockDim.x) dst[x] = val;
 	}
@@ -91,7 +108,8 @@ __global__ void __launch_bounds__(kRowThreads) k_fill_separable(S* __restrict__ 
 {
 	const int64_t rows = (int64_t)b.ny * b.nz;
 	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
-		const int y = (int)(row % b.ny), z = (int)(row / b.ny);
+		int y, z;
+		row_yz(row, b.ny, y, z);
 		const double w2 = v2[y], w3 = v3[z];
 		S* dst = u + b.i1s + (b.i2s + y) * n1 + (b.i3s + z) * n12;
 		// (((amp * v1) * v2) * v3), each product rounded in FP64, then one rounding to S
@@ -281,8 +299,9 @@ __global__ void __launch_bounds__(kRowThreads) k_update_pressure(S* __restrict__
 			C pc[kRowUnroll], pn[kRowUnroll], cf[kRowUnroll], lp[kRowUnroll];
 #pragma unroll
 			for (int k = 0; k < kRowUnroll; k++) {
-				const int64_t row = r0 + k < rows ? r0 + k : rows - 1;
-				ii[k] = (b.i1s + x) + (b.i2s + row % b.ny) * n1 + (b.i3s + row / b.ny) * n12;
+				int y, z;
+				row_yz(r0 + k < rows ? r0 + k : rows - 1, b.ny, y, z);
+				ii[k] = (b.i1s + x) + (b.i2s + y) * n1 + (b.i3s + z) * n12;
 				pc[k] = Storage<S>::load(prc[ii[k]]);
 				pn[k] = Storage<S>::load(prn[ii[k]]);
 				cf[k] = Storage<S>::load(coef[ii[k]]);
@@ -396,8 +415,7 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce(const S* __restrict__ u1
 #pragma unroll
 		for (int k = 0; k < kRowUnroll; k++) {
 			const int64_t row = r0 + k < rows ? r0 + k : rows - 1;
-			yk[k] = (int)(row % r.b.ny);
-			zk[k] = (int)(row / r.b.ny);
+			row_yz(row, r.b.ny, yk[k], zk[k]);
 			base[k] = r.b.i1s + (r.b.i2s + yk[k]) * r.n1 + (r.b.i3s + zk[k]) * r.n12;
 		}
 		for (int x = threadIdx.x; x < r.b.nx; x += blockDim.x) {
@@ -474,6 +492,7 @@ int run_reduce(const b200_layout* lay, const b200_field& u1, const b200_field* u
 	r.n1 = lay->n1;
 	r.n12 = lay->n1 * lay->n2;
 	r.b = to_box3(box);
+	if (int rc = box_rows_ok(r.b)) return rc;
 	r.s1 = u1.scale;
 	r.s2 = u2 ? u2->scale : 1.0;
 	const int blocks = row_blocks(r.b, kRowUnroll);
@@ -599,6 +618,7 @@ int b200_fill_const(const b200_layout* lay, b200_field u, const b200_box* box, d
 	if (int rc = check_box(lay, box)) return rc;
 	if (int rc = check_field(u, "u")) return rc;
 	const Box3 b = to_box3(box);
+	if (int rc = box_rows_ok(b)) return rc;
 	const double v = val / (double)u.scale;
 	return dispatch_dtype(u.dtype, [&](auto tag) {
 		using S = decltype(tag);
@@ -686,6 +706,7 @@ int b200_fill_separable(const b200_layout* lay, b200_field u, const b200_box* bo
 	double *d1, *d2, *d3;
 	if (int rc = upload_tables(box, v1, v2, v3, s, 0, &d1, &d2, &d3)) return rc;
 	const Box3 b = to_box3(box);
+	if (int rc = box_rows_ok(b)) return rc;
 	const double a = amp / (double)u.scale;
 	int rc = dispatch_dtype(u.dtype, [&](auto tag) {
 		using S = decltype(tag);
@@ -719,6 +740,7 @@ int b200_update_pressure(const b200_layout* lay, b200_field prn, b200_field prc,
 		return set_error(B200_ERR_UNSUPPORTED, "prn, prc and lapla must share one scale");
 	const b200_box box{lay->s1, lay->e1, lay->s2, lay->e2, lay->s3, lay->e3};
 	const Box3 b = to_box3(&box);
+	if (int rc = box_rows_ok(b)) return rc;
 	return dispatch_dtype(prn.dtype, [&](auto tag) {
 		using S = decltype(tag);
 		k_update_pressure<S, true><<<row_blocks(b, kRowUnroll), kRowThreads, 0, as_stream(stream)>>>(
@@ -849,6 +871,7 @@ int b200_l1_sums_separable_noalloc(const b200_layout* lay, b200_field u, const b
 	if (dtype_size(ref_dtype) == 0) return set_error(B200_ERR_ARG, "ref dtype %d", ref_dtype);
 	if (!v1 || !v2 || !v3) return set_error(B200_ERR_ARG, "NULL table");
 	const Box3 b = to_box3(box);
+	if (int rc = box_rows_ok(b)) return rc;
 	const int64_t entries = (int64_t)b.nx + b.ny + b.nz;
 	if (entries > kNoAllocTableMax)
 		return set_error(B200_ERR_UNSUPPORTED,
