@@ -182,8 +182,13 @@ def l1_sums_eigen(prn: Grid, propa: Propagator_Ac2, amp: float):
     import ctypes
     from .layout import fill_tables
     lay = prn.layout
-    p = propa.setup.params(lay)
-    tabs = fill_tables(lay, propa.setup.samp, INNER_POINTS, EIGEN_FUNCS, p)
+    # the 1-D tables depend on the grid only (the amplitude is a factor): built once per grid
+    key = (id(propa.setup), lay.n1, lay.n2, lay.n3, lay.prec)
+    cache = propa.__dict__.setdefault("_eigen_tables", {})
+    tabs = cache.get(key)
+    if tabs is None:
+        tabs = fill_tables(lay, propa.setup.samp, INNER_POINTS, EIGEN_FUNCS, propa.setup.params(lay))
+        cache[key] = tabs
     s1, s2 = ctypes.c_double(), ctypes.c_double()
     cl, box = prn.c_layout(), prn.c_box(INNER_POINTS)
     ref_dtype = _lib.DTYPE_CODE["f64" if lay.prec == "f64" else "f32"]
