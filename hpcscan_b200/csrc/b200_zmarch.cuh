@@ -266,10 +266,12 @@ struct ZCfg {
 	static constexpr int R4 = XH ? round_up(R, VA) : 0;     // x halo, whole 16-byte vectors
 	static constexpr int RY = YH ? R : 0;
 	static constexpr int RZ = ZQ ? R : 0;
-	// planes per pass of the z loop (0: four for the operators without pointwise tiles, two for
-	// the pressure updates, whose registers are the tighter; measured at 512^3 O8 on B200)
-	static constexpr int UQ = !ZQ ? 1 : UQ_ > 0 ? UQ_ : (MODE == MODE_PRESSURE || MODE == MODE_STEP ||
-	                                                     MODE == MODE_MODEL || MODE == MODE_GRAD) ? 2 : 4;
+	// planes per pass of the z loop (0: four, except two where four would spill registers: the
+	// fused step, the modelling passes, and the pressure update outside R = 3..6; four measured
+	// 1.3 % faster than two for the pressure update at 512^3 O8 on B200)
+	static constexpr int UQ = !ZQ ? 1 : UQ_ > 0 ? UQ_
+	                        : (MODE == MODE_STEP || MODE == MODE_MODEL || MODE == MODE_GRAD ||
+	                           (MODE == MODE_PRESSURE && (R < 3 || R > 6))) ? 2 : 4;
 	static constexpr int BX = TX + 2 * R4;
 	static constexpr int BY = TY + 2 * RY;
 	static constexpr int NSU = (ZONLY && 2 * PF + 4 > RZ + 1 + PF) ? 2 * PF + 4
