@@ -382,10 +382,10 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	if (threadIdx.x == 0) {
 		for (int s = 0; s < NSU; s++) {
 			mbar_init(&full_u[s], 1);
-			mbar_init(&empty_u[s], Cfg::NWC);
+			mbar_init(&empty_u[s], NC);        // every consumer thread releases
 		}
 		for (int s = 0; s < NSP; s++) {
-			mbar_init(&empty_p[s], Cfg::NWC);
+			mbar_init(&empty_p[s], NC);
 		}
 		fence_mbar_init();
 	}
@@ -587,10 +587,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 					}
 				}
 			}
-			if constexpr (Cfg::ZONLY) {
-				__syncwarp();
-				if (lane == 0) mbar_arrive(&empty_u[s]);
-			}
+			if constexpr (Cfg::ZONLY) mbar_arrive(&empty_u[s]);
 			if (j >= 2 * RZ) {
 				const int o = j - 2 * RZ;
 				const int k = z0 + o;                     // output plane
@@ -830,19 +827,15 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						}
 					}
 				}
-				__syncwarp();
-				if (lane == 0) {
-					if constexpr (!Cfg::ZONLY) mbar_arrive(&empty_u[sc]);
-					if constexpr (Cfg::P) mbar_arrive(&empty_p[rp.slot]);
-				}
+				// each thread releases the slots after its own last read of them
+				if constexpr (!Cfg::ZONLY) mbar_arrive(&empty_u[sc]);
+				if constexpr (Cfg::P) mbar_arrive(&empty_p[rp.slot]);
 				rc.advance();
 				rp.advance();
 			}
 			if constexpr (Cfg::ZQ && !Cfg::ZONLY) {
-				if (j < RZ || j >= J - RZ) {   // planes that are never a centre plane
-					__syncwarp();
-					if (lane == 0) mbar_arrive(&empty_u[s]);
-				}
+				if (j < RZ || j >= J - RZ)     // planes that are never a centre plane
+					mbar_arrive(&empty_u[s]);
 			}
 			ru.advance();
 	});
