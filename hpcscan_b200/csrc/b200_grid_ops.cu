@@ -254,6 +254,93 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_planes(S* __restrict__ u, BcA
 	}
 }
 
+// The whole anti-mirror condition in one launch, for a single-rank 3-D grid whose axes all have
+// at least 2 halo + 2 inner points (phase A's partition). Phase A reads values from before the
+// boundary planes are zeroed; here the zeroing happens in the same launch, so each point that
+// is both read and zeroed is zeroed by its only reader, after the read:
+//  * i1 faces (one (row, side, distance) per thread): the mirror point xm = s1 + k (e1 - k) is
+//    read, its halo written; xm is zeroed by this thread when it lies on an i2 or i3 boundary
+//    plane; on an i3 boundary plane within the i2 band (rows s2+1..s2+R, e2-R..e2-1) this thread
+//    also writes xm's i2 halo, which would otherwise need a second reader; the k = 1 lane zeroes
+//    the i1 boundary point of its row;
+//  * i2 faces (column (x, z)): columns with x in the i1 band on an i3 boundary plane are left to
+//    the i1 faces; the others read, write their halos, zero the i2 boundary point (outside the
+//    i1 band) and, on an i3 boundary plane, the mirror points they read;
+//  * i3 faces (column (x, y)): read, write the halos, and zero the i3 boundary point unless
+//    x is in the i1 band or on an i1 boundary line, or y in the i2 band or on an i2 line.
+// Mirror values from a boundary line an earlier face zeroes are -0 without a read, as in phase A.
+template <typename S>
+__global__ void __launch_bounds__(kBcThreads) k_bc_one(S* __restrict__ u, BcArgs a, BcPart p)
+{
+	constexpr int KMAX = 8;
+	const int R = a.halo;
+	const int ny = (int)(a.e[1] - a.s[1] + 1);
+	const int64_t s1 = a.s[0], e1 = a.e[0], s2 = a.s[1], e2 = a.e[1], s3 = a.s[2], e3 = a.e[2];
+	const int64_t n1 = a.n1, n12 = a.n12;
+	auto neg = [](S v) { return Storage<S>::store(-Storage<S>::load(v)); };
+	auto xband = [&](int64_t x) { return (x > s1 && x <= s1 + R) || (x < e1 && x >= e1 - R); };
+	auto yband = [&](int64_t y) { return (y > s2 && y <= s2 + R) || (y < e2 && y >= e2 - R); };
+	int b = blockIdx.x;
+	if (b < p.nbx) {
+		const int lane = threadIdx.x % p.lanes, rib = threadIdx.x / p.lanes;
+		if (rib >= kBcThreads / p.lanes) return;
+		const int side = lane / R, k = lane % R + 1;
+		const int row = b * (kBcThreads / p.lanes) + rib;
+		if (row >= ny * (int)(e3 - s3 + 1)) return;
+		const int64_t y = s2 + row % ny, z = s3 + row / ny;
+		const int64_t base = y * n1 + z * n12;
+		const int64_t xm = side ? e1 - k : s1 + k;
+		const S v = u[base + xm];
+		u[base + (side ? e1 + k : s1 - k)] = neg(v);
+		const bool yplane = y == s2 || y == e2, zplane = z == s3 || z == e3;
+		if (zplane && yband(y)) u[(y <= s2 + R ? 2 * s2 - y : 2 * e2 - y) * n1 + z * n12 + xm] = neg(v);
+		if (yplane || zplane) u[base + xm] = S(0.0f);
+		if (k == 1) u[base + (side ? e1 : s1)] = S(0.0f);
+		return;
+	}
+	b -= p.nbx;
+	const int axis = (b < p.nby) ? 1 : 2;
+	if (axis == 2) b -= p.nby;
+	const int chunk = b % p.nchunk;
+	const int r = b / p.nchunk;
+	const int side = r % 2;
+	const int line = r / 2;
+	const int x = chunk * kBcThreads + threadIdx.x;
+	if (s1 + x > e1) return;
+	const int64_t i1 = s1 + x;
+	const bool xline = i1 == s1 || i1 == e1;
+	S mv[KMAX];
+	if (axis == 1) {
+		const int64_t i3 = s3 + line;
+		const bool zplane = i3 == s3 || i3 == e3, xb = xband(i1);
+		if (zplane && xb) return;
+		const int64_t col = i1 + i3 * n12, bnd = side ? e2 : s2;
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R) mv[k - 1] = xline ? S(0.0f) : u[col + (side ? bnd - k : bnd + k) * n1];
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R) u[col + (side ? bnd + k : bnd - k) * n1] = neg(mv[k - 1]);
+		if (!xb) u[col + bnd * n1] = S(0.0f);
+		if (zplane) {
+#pragma unroll
+			for (int k = 1; k <= KMAX; k++)
+				if (k <= R) u[col + (side ? bnd - k : bnd + k) * n1] = S(0.0f);
+		}
+	} else {
+		const int64_t i2 = s2 + line;
+		const bool yline = i2 == s2 || i2 == e2;
+		const int64_t col = i1 + i2 * n1, bnd = side ? e3 : s3;
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R) mv[k - 1] = (xline || yline) ? S(0.0f) : u[col + (side ? bnd - k : bnd + k) * n12];
+#pragma unroll
+		for (int k = 1; k <= KMAX; k++)
+			if (k <= R) u[col + (side ? bnd + k : bnd - k) * n12] = neg(mv[k - 1]);
+		if (!(xline || yline || xband(i1) || yband(i2))) u[col + bnd * n12] = S(0.0f);
+	}
+}
+
 // Sequential form for tiny grids (an axis with fewer than halo + 2 inner points): one face
 // per launch in the reference order, each thread owning one line normal to the face.
 template <typename S>
@@ -577,6 +664,12 @@ int apply_boundary(const b200_layout* lay, const b200_field& u, int bc_type, int
 			return B200_OK;
 		}
 		const BcPart ph = bc_partition(a, false), pp = bc_partition(a, true);
+		bool one = lay->dim == 3 && a.faces == 0x3F;
+		for (int d = 0; d < 3; d++) one = one && (a.e[d] - a.s[d] + 1) >= 2 * a.halo + 2;
+		if (one) {
+			k_bc_one<S><<<ph.nbx + ph.nby + ph.nbz, kBcThreads, 0, s>>>(p, a, ph);
+			return check_launch("k_bc_one");
+		}
 		k_bc_halos<S><<<ph.nbx + ph.nby + ph.nbz, kBcThreads, 0, s>>>(p, a, ph);
 		if (int rc = check_launch("k_bc_halos")) return rc;
 		k_bc_planes<S><<<pp.nbx + pp.nby + pp.nbz, kBcThreads, 0, s>>>(p, a, pp);
