@@ -59,10 +59,11 @@ def parse_args():
                    help="time steps of the bounded reference CPU sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--workload", default="propa",
-                   choices=["propa", "adjoint", "modeling", "mixed", "fd"],
+                   choices=["propa", "adjoint", "modeling", "mixed", "fd", "sustained"],
                    help="propa (default, the headline), adjoint (batched checkpointed gradients), "
-                        "modeling (batched uneven forward shots), mixed (16-bit wavefields) or "
-                        "fd (the FD_D1 / FD_D2 operator test cases)")
+                        "modeling (batched uneven forward shots), mixed (16-bit wavefields), "
+                        "fd (the FD_D1 / FD_D2 operator test cases) or sustained (the headline "
+                        "step back to back for --nt steps, with clocks and power per bin)")
     p.add_argument("--shots", type=int, default=0, help="shots (adjoint: 16, modeling: 64)")
     p.add_argument("--nt", type=int, default=0, help="time steps (adjoint: 2000, modeling: 1500)")
     p.add_argument("--checkpoint", type=int, default=45, help="adjoint checkpoint interval")
@@ -119,7 +120,7 @@ class ClockSampler:
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.samples = []          # (t, sm_mhz, max_mhz, reasons bitmask)
+        self.samples = []          # (t, sm_mhz, reasons bitmask, power_w)
         self.window = None
         self.ok = False
         self.stop_ev = threading.Event()
@@ -145,7 +146,8 @@ class ClockSampler:
             try:
                 sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
                 rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
-                self.samples.append((time.perf_counter(), sm, rs))
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                self.samples.append((time.perf_counter(), sm, rs, pw))
             except Exception:
                 pass
             time.sleep(self.PERIOD_S)
@@ -160,21 +162,33 @@ class ClockSampler:
     def __exit__(self, *a):
         self.stop_ev.set()
 
-    def summary(self):
-        if not self.ok:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+    def _reasons(self, sel):
         nv = self.nv
-        t0, t1 = self.window
-        sel = [x for x in self.samples if t0 - self.PERIOD_S <= x[0] <= t1 + self.PERIOD_S]
-        if not sel:
-            sel = self.samples[-3:]
         names = {"hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
                  "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
                  "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
                  "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4)}
-        reasons = sorted({n for _, _, rs in sel for n, bit in names.items() if rs & bit})
+        return sorted({n for x in sel for n, bit in names.items() if x[2] & bit})
+
+    def summary(self):
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        t0, t1 = self.window
+        sel = [x for x in self.samples if t0 - self.PERIOD_S <= x[0] <= t1 + self.PERIOD_S]
+        if not sel:
+            sel = self.samples[-3:]
         return {"sm_mhz": statistics.median([x[1] for x in sel]), "sm_max_mhz": self.max_mhz,
-                "reasons": reasons, "samples": len(sel)}
+                "reasons": self._reasons(sel), "samples": len(sel)}
+
+    def between(self, t0, t1):
+        """Median SM clock, mean board power (NVML's own running average) and the reasons
+        seen in the samples taken between host times t0 and t1."""
+        sel = [x for x in self.samples if t0 <= x[0] <= t1] if self.ok else []
+        if not sel:
+            return {"sm_mhz": None, "power_w": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median([x[1] for x in sel]),
+                "power_w": round(statistics.mean([x[3] for x in sel]), 1),
+                "reasons": self._reasons(sel), "samples": len(sel)}
 
 
 # ---- reference CPU path -------------------------------------------------------------------------
@@ -812,6 +826,92 @@ def fd_arm(a):
     print(json.dumps(line))
 
 
+def sustained_arm(a):
+    """The headline step (boundary condition + pressure update, 512^3 O8 FP32 eigen mode) run
+    back to back for --nt steps (default 3000, about 1.3 s), timed in bins of 100 steps with
+    CUDA events, with the SM clock, board power and clock-event reasons sampled through NVML in
+    each bin. On a 1000 W B200 this shows the power cap: after about 100 ms of back-to-back
+    steps the SM clock falls below its maximum (reason sw_power_cap) and the step time rises
+    with it, since the kernel's time follows the SM clock at that point."""
+    import torch
+
+    from hpcscan_b200 import layout as L
+    from hpcscan_b200.grid import init_device
+    from hpcscan_b200.propagator import Propagator_Ac2
+
+    init_device(0)
+    lay = L.b200_layout(3, a.size, a.size, a.size, order=a.order, prec="f32")
+    propa = Propagator_Ac2(lay)
+    propa.initialize(ratio_cfl=0.8, nt=1, snap_inc=1, modes=(1, 1, 1))
+    prn, prc = propa.prnGrid, propa.prcGrid
+    stream = torch.cuda.current_stream()
+    bin_steps = 100
+    nbins = max(1, (a.nt or 3000) // bin_steps)
+    nt = nbins * bin_steps
+
+    def step():
+        nonlocal prn, prc
+        prc.applyBoundaryCondition()
+        propa.computePressureWithFD(prn, prc)
+        prn, prc = prc, prn
+
+    bins = []
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for _ in range(a.warmup):
+            step()
+        torch.cuda.synchronize()
+        time.sleep(1.0)                  # the board back at rest after the set-up
+        for _ in range(nbins):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(stream)
+            for _ in range(bin_steps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            bins.append((e0.elapsed_time(e1) / bin_steps, clk.between(t0, t1)))
+    st = ctypes_status()
+    if st:
+        raise RuntimeError(f"device-side error word {st}")
+    pts = lay.inner_points
+    total_ms = sum(ms for ms, _ in bins) * bin_steps
+    tail = bins[len(bins) // 2:]
+    seen = sorted({r for _, c in bins for r in c["reasons"]})
+    line = {
+        "metric": f"Propa GPoint/s sustained (O{a.order} FP32 {a.size}^3, {nt} back-to-back steps)",
+        "value": round(pts * nt / (total_ms * 1e-3) / 1e9, 4), "unit": UNIT, "n_gpus": 1,
+        "steps": nt, "warmup": a.warmup, "ms_per_step": round(total_ms / nt, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (eigen mode, the reference's Propa initialisation)",
+        "config": {"workload": f"Propa Ac2Standard O{a.order} FP32 {a.size}^3 eigen mode, "
+                               "steps back to back, timed in bins", "bin_steps": bin_steps,
+                   "l2": "inputs larger than L2"},
+        "gpu_launches": (2 if min(lay.n_inner) >= 2 * lay.halo + 2 else 3) * nt,
+        "first_bin": {"ms_per_step": round(bins[0][0], 5), **bins[0][1]},
+        "second_half": {"ms_per_step": round(statistics.mean(ms for ms, _ in tail), 5),
+                        "sm_mhz": statistics.median([c["sm_mhz"] for _, c in tail
+                                                     if c["sm_mhz"] is not None] or [0]),
+                        "power_w_max": max([c["power_w"] for _, c in tail
+                                            if c["power_w"] is not None] or [0])},
+        "reasons_seen": seen,
+        "bins": [[round(ms, 5), c["sm_mhz"], c["power_w"], c["reasons"]] for ms, c in bins],
+        "bins_columns": ["ms_per_step", "sm_mhz (median)", "power_w (NVML running average)",
+                         "reasons"],
+    }
+    print(json.dumps(line))
+
+
+def ctypes_status():
+    """The library's device-side error word (non-zero: a bounded wait ran out)."""
+    import ctypes
+
+    from hpcscan_b200 import _lib
+    st = ctypes.c_int()
+    _lib.call("b200_device_status", ctypes.byref(st), 1)
+    return st.value
+
+
 def main():
     a = parse_args()
     if a.workload != "propa":
@@ -820,12 +920,13 @@ def main():
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
                                   "adjoint and no batched modelling path (fd: its CacheBlk "
-                                  "numbers are in the b200 line)"}))
+                                  "numbers are in the b200 line; sustained: the reference CPU "
+                                  "path of this step is the propa workload's reference line)"}))
             return
         if world > 1 and rank != 0:
             return
         {"adjoint": adjoint_arm, "modeling": modeling_arm, "mixed": mixed_arm,
-         "fd": fd_arm}[a.workload](a)
+         "fd": fd_arm, "sustained": sustained_arm}[a.workload](a)
         return
     if a.impl == "reference":
         reference_arm(a)

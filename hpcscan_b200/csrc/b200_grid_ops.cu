@@ -269,25 +269,32 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_planes(S* __restrict__ u, BcA
 //  * i3 faces (column (x, y)): read, write the halos, and zero the i3 boundary point unless
 //    x is in the i1 band or on an i1 boundary line, or y in the i2 band or on an i2 line.
 // Mirror values from a boundary line an earlier face zeroes are -0 without a read, as in phase A.
-template <typename S>
-__global__ void __launch_bounds__(kBcThreads) k_bc_one(S* __restrict__ u, BcArgs a, BcPart p)
+//
+// Launch grid (nbx + 4 nchunk, max(ny, nz)), the halo width R a template parameter so that every
+// index comes from constant divisions: blockIdx.y is the line (i3 - s3 for the i1 and i2 faces,
+// i2 - s2 for the i3 faces) and blockIdx.x the part:
+//   [0, nbx)                      i1 faces of plane i3: 2R lanes (side, k) per i2 row,
+//                                 kBcThreads / 2R rows per block
+//   [nbx, nbx + 2 nchunk)         i2 faces of plane i3: one run of kBcThreads i1 per (run, side)
+//   [nbx + 2 nchunk, + 2 nchunk)  i3 faces of row i2: the same runs
+template <typename S, int R>
+__global__ void __launch_bounds__(kBcThreads) k_bc_one(S* __restrict__ u, BcArgs a, int nbx, int nchunk)
 {
-	constexpr int KMAX = 8;
-	const int R = a.halo;
-	const int ny = (int)(a.e[1] - a.s[1] + 1);
+	constexpr int L = 2 * R, RPB = kBcThreads / L;
+	const int ny = (int)(a.e[1] - a.s[1] + 1), nz = (int)(a.e[2] - a.s[2] + 1);
 	const int64_t s1 = a.s[0], e1 = a.e[0], s2 = a.s[1], e2 = a.e[1], s3 = a.s[2], e3 = a.e[2];
 	const int64_t n1 = a.n1, n12 = a.n12;
 	auto neg = [](S v) { return Storage<S>::store(-Storage<S>::load(v)); };
 	auto xband = [&](int64_t x) { return (x > s1 && x <= s1 + R) || (x < e1 && x >= e1 - R); };
 	auto yband = [&](int64_t y) { return (y > s2 && y <= s2 + R) || (y < e2 && y >= e2 - R); };
-	int b = blockIdx.x;
-	if (b < p.nbx) {
-		const int lane = threadIdx.x % p.lanes, rib = threadIdx.x / p.lanes;
-		if (rib >= kBcThreads / p.lanes) return;
+	const int line = (int)blockIdx.y;
+	int b = (int)blockIdx.x;
+	if (b < nbx) {
+		const int rib = (int)threadIdx.x / L, lane = (int)threadIdx.x % L;
+		const int yr = b * RPB + rib;
+		if (rib >= RPB || yr >= ny || line >= nz) return;
 		const int side = lane / R, k = lane % R + 1;
-		const int row = b * (kBcThreads / p.lanes) + rib;
-		if (row >= ny * (int)(e3 - s3 + 1)) return;
-		const int64_t y = s2 + row % ny, z = s3 + row / ny;
+		const int64_t y = s2 + yr, z = s3 + line;
 		const int64_t base = y * n1 + z * n12;
 		const int64_t xm = side ? e1 - k : s1 + k;
 		const S v = u[base + xm];
@@ -298,46 +305,70 @@ __global__ void __launch_bounds__(kBcThreads) k_bc_one(S* __restrict__ u, BcArgs
 		if (k == 1) u[base + (side ? e1 : s1)] = S(0.0f);
 		return;
 	}
-	b -= p.nbx;
-	const int axis = (b < p.nby) ? 1 : 2;
-	if (axis == 2) b -= p.nby;
-	const int chunk = b % p.nchunk;
-	const int r = b / p.nchunk;
-	const int side = r % 2;
-	const int line = r / 2;
-	const int x = chunk * kBcThreads + threadIdx.x;
+	b -= nbx;
+	const int axis = (b < 2 * nchunk) ? 1 : 2;
+	if (axis == 2) b -= 2 * nchunk;
+	const int side = b & 1, chunk = b >> 1;
+	if (line >= (axis == 1 ? nz : ny)) return;
+	const int x = chunk * kBcThreads + (int)threadIdx.x;
 	if (s1 + x > e1) return;
 	const int64_t i1 = s1 + x;
 	const bool xline = i1 == s1 || i1 == e1;
-	S mv[KMAX];
+	S mv[R];
 	if (axis == 1) {
 		const int64_t i3 = s3 + line;
 		const bool zplane = i3 == s3 || i3 == e3, xb = xband(i1);
 		if (zplane && xb) return;
 		const int64_t col = i1 + i3 * n12, bnd = side ? e2 : s2;
 #pragma unroll
-		for (int k = 1; k <= KMAX; k++)
-			if (k <= R) mv[k - 1] = xline ? S(0.0f) : u[col + (side ? bnd - k : bnd + k) * n1];
+		for (int k = 1; k <= R; k++) mv[k - 1] = xline ? S(0.0f) : u[col + (side ? bnd - k : bnd + k) * n1];
 #pragma unroll
-		for (int k = 1; k <= KMAX; k++)
-			if (k <= R) u[col + (side ? bnd + k : bnd - k) * n1] = neg(mv[k - 1]);
+		for (int k = 1; k <= R; k++) u[col + (side ? bnd + k : bnd - k) * n1] = neg(mv[k - 1]);
 		if (!xb) u[col + bnd * n1] = S(0.0f);
 		if (zplane) {
 #pragma unroll
-			for (int k = 1; k <= KMAX; k++)
-				if (k <= R) u[col + (side ? bnd - k : bnd + k) * n1] = S(0.0f);
+			for (int k = 1; k <= R; k++) u[col + (side ? bnd - k : bnd + k) * n1] = S(0.0f);
 		}
 	} else {
 		const int64_t i2 = s2 + line;
 		const bool yline = i2 == s2 || i2 == e2;
 		const int64_t col = i1 + i2 * n1, bnd = side ? e3 : s3;
 #pragma unroll
-		for (int k = 1; k <= KMAX; k++)
-			if (k <= R) mv[k - 1] = (xline || yline) ? S(0.0f) : u[col + (side ? bnd - k : bnd + k) * n12];
+		for (int k = 1; k <= R; k++)
+			mv[k - 1] = (xline || yline) ? S(0.0f) : u[col + (side ? bnd - k : bnd + k) * n12];
 #pragma unroll
-		for (int k = 1; k <= KMAX; k++)
-			if (k <= R) u[col + (side ? bnd + k : bnd - k) * n12] = neg(mv[k - 1]);
+		for (int k = 1; k <= R; k++) u[col + (side ? bnd + k : bnd - k) * n12] = neg(mv[k - 1]);
 		if (!(xline || yline || xband(i1) || yband(i2))) u[col + bnd * n12] = S(0.0f);
+	}
+}
+
+// k_bc_one for halo widths 1..8 (FD orders 2..16); *handled stays 0 for other widths and for
+// grids beyond the launch's line limit, which take the two-launch form.
+template <typename S>
+int launch_bc_one(S* u, const BcArgs& a, cudaStream_t s, int* handled)
+{
+	*handled = 0;
+	const int64_t nx = a.e[0] - a.s[0] + 1, ny = a.e[1] - a.s[1] + 1, nz = a.e[2] - a.s[2] + 1;
+	if (a.halo < 1 || a.halo > 8 || ny > 65535 || nz > 65535) return B200_OK;
+	*handled = 1;
+	const int nchunk = (int)((nx + kBcThreads - 1) / kBcThreads);
+	auto go = [&](auto rt) {
+		constexpr int R = decltype(rt)::value;
+		constexpr int RPB = kBcThreads / (2 * R);
+		const int nbx = (int)((ny + RPB - 1) / RPB);
+		const dim3 grd(nbx + 4 * nchunk, (unsigned)(ny > nz ? ny : nz));
+		k_bc_one<S, R><<<grd, kBcThreads, 0, s>>>(u, a, nbx, nchunk);
+		return check_launch("k_bc_one");
+	};
+	switch (a.halo) {
+	case 1: return go(std::integral_constant<int, 1>{});
+	case 2: return go(std::integral_constant<int, 2>{});
+	case 3: return go(std::integral_constant<int, 3>{});
+	case 4: return go(std::integral_constant<int, 4>{});
+	case 5: return go(std::integral_constant<int, 5>{});
+	case 6: return go(std::integral_constant<int, 6>{});
+	case 7: return go(std::integral_constant<int, 7>{});
+	default: return go(std::integral_constant<int, 8>{});
 	}
 }
 
@@ -667,8 +698,9 @@ int apply_boundary(const b200_layout* lay, const b200_field& u, int bc_type, int
 		bool one = lay->dim == 3 && a.faces == 0x3F;
 		for (int d = 0; d < 3; d++) one = one && (a.e[d] - a.s[d] + 1) >= 2 * a.halo + 2;
 		if (one) {
-			k_bc_one<S><<<ph.nbx + ph.nby + ph.nbz, kBcThreads, 0, s>>>(p, a, ph);
-			return check_launch("k_bc_one");
+			int handled = 0;
+			const int rc = launch_bc_one<S>(p, a, s, &handled);
+			if (handled) return rc;
 		}
 		k_bc_halos<S><<<ph.nbx + ph.nby + ph.nbz, kBcThreads, 0, s>>>(p, a, ph);
 		if (int rc = check_launch("k_bc_halos")) return rc;
