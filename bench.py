@@ -1,6 +1,6 @@
 """Benchmark of the hpcscan B200 hot path: the Propa acoustic propagator step.
 
-Workload (BASELINE north-star configuration): Propa Ac2Standard, FD order 8, FP32,
+Workload (the headline configuration): Propa Ac2Standard, FD order 8, FP32,
 n1 = n2 = n3 = 512 inner points (520^3 with halos), eigen mode (1, 1, 1), ratioCFL 0.8.
 A step is one time step of Propagator_Ac2::computeWavefieldNextTimeStep:
 applyBoundaryCondition(prc) then computePressureWithFD(prn, prc), then the swap.
