@@ -232,7 +232,11 @@ def test_array_ops_bitexact(gpu, prec):
 
 BC_LAYOUTS = [L.b200_layout(3, 30, 21, 22, order=8), L.reference_layout(3, 25, 20, 21, order=16),
               L.b200_layout(3, 12, 9, 10, order=16, prec="f64"),      # small: sequential faces
-              L.reference_layout(2, 33, 20, order=4, prec="f64"), L.reference_layout(1, 40, order=6)]
+              L.reference_layout(2, 33, 20, order=4, prec="f64"), L.reference_layout(1, 40, order=6),
+              # the one-launch form at the other halo widths, several i1 runs, ny != nz
+              L.b200_layout(3, 300, 17, 40, order=2), L.reference_layout(3, 37, 26, 19, order=6),
+              L.b200_layout(3, 40, 33, 27, order=10, prec="f64"), L.b200_layout(3, 35, 30, 31, order=14),
+              L.b200_layout(3, 530, 18, 19, order=12)]
 
 
 @pytest.mark.parametrize("lay", BC_LAYOUTS, ids=lay_id)
