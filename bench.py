@@ -21,6 +21,10 @@ device time is the max over ranks, and value = all points updated / that time.
   cpu_baseline   the reference CPU path itself (oracle/_ref/hpcscan_fp32, test mode
                  CacheBlk, all host threads) on a bounded number of steps of the same grid
 --impl reference prints the same line for the reference CPU implementation.
+
+The other workloads (--workload) print their own line: adjoint and modeling split their
+fixed survey of shots over the ranks under torchrun (one GPU per rank, the adjoint's survey
+gradient summed by one all-reduce); mixed, fd and sustained run on rank 0.
 """
 from __future__ import annotations
 
@@ -457,6 +461,33 @@ def e2e_job(a, lay, device):
 
 # ---- batched modelling and adjoint workloads ------------------------------------------------------
 
+def _shot_dist():
+    """Process group of the shot-parallel workloads under torchrun (NCCL, one GPU per rank):
+    (dist or None, rank, world, local rank)."""
+    rank, world, local = dist_env()
+    if world == 1:
+        return None, rank, world, local
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                            device_id=torch.device(f"cuda:{local}"))
+    return dist, rank, world, local
+
+
+def sum_over_ranks(dist, values, device):
+    """Per-rank counts -> their sums over all ranks (one all-reduce); the values themselves on
+    a single process."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.tolist()
+
+
 def _surface_shots(n, nshot, seed):
     """Distinct seeded source positions on the surface plane i1 = 1, off the receiver lattice."""
     import numpy as np
@@ -493,21 +524,32 @@ def adjoint_arm(a):
     the squared slowness (sigma 10 points, centre); gradient of 1/2 |d - dobs|^2 with respect to
     the squared slowness at the background; checkpoints every 45 steps. Batched: all shots in
     each launch, the whole gradient (forward, then segment-wise recompute, adjoint and
-    gradient) replayed from one CUDA graph. Plain: the same kernels one shot per launch, from
-    the host, no graph. Both give bit-identical gradients (checked)."""
+    gradient) replayed from one CUDA graph, then the survey gradient (the sum over the shots).
+    Plain: the same kernels one shot per launch, from the host, no graph. Both give
+    bit-identical per-shot gradients (checked).
+
+    Under torchrun the survey is split over the ranks (hpcscan_b200.shots: one GPU per rank,
+    its shots in one batch, nothing exchanged in the time loop) and the survey gradient ends
+    with one sum all-reduce, inside the timed region; the time is the max over ranks (strong
+    scaling: the survey is fixed). The plain form runs on a single process only."""
     import numpy as np
     import torch
 
     from hpcscan_b200.grid import init_device
     from hpcscan_b200.modeling import Batch, Shot, grf_velocity, run_graph, stable_dt
+    from hpcscan_b200.shots import my_shots, survey_gradient
 
+    dist, rank, world, local = _shot_dist()
     n = a.size if a.size != 512 else 256
     nshot = a.shots or 16
+    if nshot < world:
+        raise SystemExit(f"{nshot} shots for {world} ranks: every rank needs a shot")
     nt = a.nt or 2000
     order, dx, f0 = a.order, 10.0, 10.0
-    init_device(0)
-    dev = "cuda:0"
-    vel0 = grf_velocity((n, n, n), sigma=20.0, seed=1234)
+    init_device(local)
+    dev = f"cuda:{local}"
+    mine = my_shots([1.0] * nshot, rank, world)
+    vel0 = grf_velocity((n, n, n), sigma=20.0, seed=1234, device=local)
     c = (n - 1) / 2.0
     ax = torch.arange(n, device=dev, dtype=torch.float32)
     r2 = (ax[:, None, None] - c) ** 2 + (ax[None, :, None] - c) ** 2 + (ax[None, None, :] - c) ** 2
@@ -518,47 +560,63 @@ def adjoint_arm(a):
     dt = stable_dt(order, dx, 4500.0)
 
     def shots(vel, dobs=None):
-        return [Shot(n=(n, n, n), dx=dx, vel=vel, src=s, rec=rec, amp=1.0, sponge=20,
-                     dobs=None if dobs is None else dobs[i]) for i, s in enumerate(srcs)]
+        return [Shot(n=(n, n, n), dx=dx, vel=vel, src=srcs[i], rec=rec, amp=1.0, sponge=20,
+                     dobs=None if dobs is None else dobs[j]) for j, i in enumerate(mine)]
 
-    obs = Batch(shots(vel_true), order, dt, nt, f0)
+    obs = Batch(shots(vel_true), order, dt, nt, f0, device=local)
     obs.forward()
     torch.cuda.synchronize()
-    dobs = [obs.traces(i).clone() for i in range(nshot)]
+    dobs = [obs.traces(j).clone() for j in range(len(mine))]
     obs.close()
     del obs
     torch.cuda.empty_cache()
 
-    # batched: one graph for the whole gradient of all shots
-    bat = Batch(shots(vel0, dobs), order, dt, nt, f0, gradient=True, checkpoint=a.checkpoint)
+    # batched: one graph for the whole gradient of this rank's shots, then the survey gradient
+    bat = Batch(shots(vel0, dobs), order, dt, nt, f0, gradient=True, checkpoint=a.checkpoint,
+                device=local)
+    gsum = torch.empty((n, n, n), dtype=torch.float32, device=dev)
     mem_batched = torch.cuda.memory_allocated() / 1e9
     ctas = bat.ctas_per_pass
     g = run_graph(lambda s: (bat.forward(s), bat.backward(s)))
-    t_batched = _timed(g.replay, reps=1)          # warm-up replay
-    t_batched = _timed(g.replay, reps=1)
-    launches = bat.launches
-    grads = [bat.states[i].grad.clone() for i in range(nshot)]
-    J = [bat.misfit(i) for i in range(nshot)]
+
+    def job():
+        g.replay()
+        survey_gradient(bat, out=gsum)
+
+    _timed(job)                                    # warm-up replay
+    t_batched = _timed(job)
+    (t_batched,) = max_over_ranks(dist, [t_batched], dev)
+    launches, jsum = sum_over_ranks(dist, [bat.launches, sum(bat.misfit(j) for j in range(len(mine)))], dev)
+    grads = [bat.states[j].grad.clone() for j in range(len(mine))] if world == 1 else []
+    gnorm = float(gsum.double().norm())
     del g
     bat.close()
     del bat
     torch.cuda.empty_cache()
 
-    # plain: one shot per launch, eager, shot after shot; each shot's set-up (allocation, tensor
-    # maps) stays outside the timed part, which is its forward + backward pass
-    def plain_one(i):
-        b = Batch(shots(vel0, dobs)[i:i + 1], order, dt, nt, f0, gradient=True,
-                  checkpoint=a.checkpoint)
-        sec = _timed(lambda: (b.forward(), b.backward()))
-        out = b.states[0].grad.clone()
-        b.close()
-        return sec, out
-    plain_one(0)                                   # warm-up
-    t_plain, same = 0.0, True
-    for i in range(nshot):
-        sec, gi = plain_one(i)
-        t_plain += sec
-        same = same and bool(torch.equal(gi, grads[i]))
+    plain = None
+    if world == 1:
+        # plain: one shot per launch, eager, shot after shot; each shot's set-up (allocation,
+        # tensor maps) stays outside the timed part, which is its forward + backward pass
+        def plain_one(i):
+            b = Batch(shots(vel0, dobs)[i:i + 1], order, dt, nt, f0, gradient=True,
+                      checkpoint=a.checkpoint, device=local)
+            sec = _timed(lambda: (b.forward(), b.backward()))
+            out = b.states[0].grad.clone()
+            b.close()
+            return sec, out
+        plain_one(0)                                   # warm-up
+        t_plain, same = 0.0, True
+        for i in range(nshot):
+            sec, gi = plain_one(i)
+            t_plain += sec
+            same = same and bool(torch.equal(gi, grads[i]))
+        plain = (t_plain, same)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
 
     pts = n ** 3
     k = a.checkpoint
@@ -567,32 +625,38 @@ def adjoint_arm(a):
     # 20 B; checkpoint save (8 B/pt written) and restore (8 B read + 8 B written) per checkpoint
     alg = pts * (16 * nt + 16 * (nt - nck) + 16 * nt + 20 * nt + 24 * nck) * nshot
     peak, peak_src = measured_peak()
+    peak_job = peak * world
     line = {
         "metric": f"adjoint gradient shots/s ({n}^3, O{order} FP32, {nt} steps, checkpoint {k})",
-        "value": round(nshot / t_batched, 4), "unit": "shots/s", "n_gpus": 1, "steps": nt,
+        "value": round(nshot / t_batched, 4), "unit": "shots/s", "n_gpus": world, "steps": nt,
         "warmup": 1, "ms_per_step": round(t_batched / nt * 1e3, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Gaussian-random-field velocity 1500-4500 m/s, 5 % Gaussian "
                 "anomaly of the squared slowness, Ricker 10 Hz sources); no dataset involved",
         "config": {"workload": "batched checkpointed adjoint gradients", "n": n, "shots": nshot,
                    "order": order, "dx_m": dx, "receivers": len(rec), "sponge": 20,
                    "checkpoint_every": k, "ctas_per_pass": ctas,
+                   "parallelism": f"shots over {world} rank(s), one gradient all-reduce",
                    "device_memory_gb": round(mem_batched, 1)},
-        "plain": {"value": round(nshot / t_plain, 4), "unit": "shots/s",
-                  "form": "same kernels, one shot per launch, eager host loop, no CUDA graph "
-                          "(per-shot set-up not timed)",
-                  "seconds": round(t_plain, 3)},
-        "speedup_vs_plain": round(t_plain / t_batched, 3),
-        "gradients_identical_to_plain": same,
-        "misfit_mean": float(np.mean(J)),
-        "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "achieved": round(alg / t_batched / 1e9, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(alg / t_batched / 1e9 / peak, 4),
-                     "peak_source": peak_src,
+        "misfit_mean": jsum / nshot,
+        "survey_gradient_norm": gnorm,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": round(alg / t_batched / 1e9, 1),
+                     "peak": peak_job, "unit": "GB/s",
+                     "frac": round(alg / t_batched / 1e9 / peak_job, 4),
+                     "peak_source": peak_src + (f" x {world} GPUs" if world > 1 else ""),
                      "alg_bytes": "per shot-step: 16 forward + 16 recompute + 16 adjoint + 20 "
                                   "gradient, plus checkpoint save/restore"},
         "seconds": round(t_batched, 3),
     }
+    if plain is not None:
+        t_plain, same = plain
+        line["plain"] = {"value": round(nshot / t_plain, 4), "unit": "shots/s",
+                         "form": "same kernels, one shot per launch, eager host loop, no CUDA "
+                                 "graph (per-shot set-up not timed)",
+                         "seconds": round(t_plain, 3)}
+        line["speedup_vs_plain"] = round(t_plain / t_batched, 3)
+        line["gradients_identical_to_plain"] = same
     print(json.dumps(line))
 
 
@@ -601,64 +665,90 @@ def modeling_arm(a):
     63) (128 .. 320), dx 10 m, Gaussian-random-field velocity 1500-4500 m/s (seed 1234 + s,
     Gaussian kernel sigma 20 points), Ricker 10 Hz point source at the surface centre (i1 = 1),
     20-point sponge, O8 FP32, 1500 steps; every step of every shot in one launch, the time loop
-    in one CUDA graph; against the same kernels one shot per launch without a graph."""
+    in one CUDA graph; against the same kernels one shot per launch without a graph.
+
+    Under torchrun the survey is split over the ranks by work (hpcscan_b200.shots: points per
+    shot, longest first to the least-loaded rank), each rank's shots in one batch on its GPU,
+    nothing exchanged; the time is the max over ranks (strong scaling: the survey is fixed).
+    The plain form runs on a single process only."""
     import numpy as np
     import torch
 
     from hpcscan_b200.grid import init_device
     from hpcscan_b200.modeling import Batch, Shot, grf_velocity, run_graph, stable_dt
+    from hpcscan_b200.shots import my_shots
 
+    dist, rank, world, local = _shot_dist()
     nshot = a.shots or 64
+    if nshot < world:
+        raise SystemExit(f"{nshot} shots for {world} ranks: every rank needs a shot")
     nt = a.nt or 1500
     order, dx, f0 = a.order, 10.0, 10.0
-    init_device(0)
+    init_device(local)
     sizes = [128 + round(192 * s / max(nshot - 1, 1)) for s in range(nshot)]
+    mine = my_shots([float(n) ** 3 for n in sizes], rank, world)
     dt = stable_dt(order, dx, 4500.0)
     shots = []
-    for s, n in enumerate(sizes):
-        vel = grf_velocity((n, n, n), sigma=20.0, seed=1234 + s)
+    for s in mine:
+        n = sizes[s]
+        vel = grf_velocity((n, n, n), sigma=20.0, seed=1234 + s, device=local)
         rec = np.array([(1, j, n // 2) for j in range(0, n, 2)])
         shots.append(Shot(n=(n, n, n), dx=dx, vel=vel, src=(1, n // 2, n // 2), rec=rec,
                           amp=1.0, sponge=20))
-    bat = Batch(shots, order, dt, nt, f0)
+    bat = Batch(shots, order, dt, nt, f0, device=local)
     g = run_graph(lambda st: bat.forward(st))
     _timed(g.replay)
     t_batched = _timed(g.replay)
-    traces = [bat.traces(i).clone() for i in range(nshot)]
-    launches = bat.launches // 2
+    dev = f"cuda:{local}"
+    (t_batched,) = max_over_ranks(dist, [t_batched], dev)
+    (launches,) = sum_over_ranks(dist, [bat.launches // 2], dev)
+    traces = [bat.traces(j).clone() for j in range(len(mine))] if world == 1 else []
     del g
     bat.close()
     del bat
     torch.cuda.empty_cache()
-    same, t_plain = True, 0.0
-    for i in range(nshot):
-        b = Batch(shots[i:i + 1], order, dt, nt, f0)
-        t_plain += _timed(b.forward)
-        same = same and bool(torch.equal(b.traces(0), traces[i]))
-        b.close()
+    plain = None
+    if world == 1:
+        same, t_plain = True, 0.0
+        for i in range(nshot):
+            b = Batch(shots[i:i + 1], order, dt, nt, f0, device=local)
+            t_plain += _timed(b.forward)
+            same = same and bool(torch.equal(b.traces(0), traces[i]))
+            b.close()
+        plain = (t_plain, same)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     pts = sum(n ** 3 for n in sizes) * nt
     peak, peak_src = measured_peak()
+    peak_job = peak * world
     line = {
         "metric": f"batched modelling GPoint/s ({nshot} shots 128^3..320^3, O{order} FP32, {nt} steps)",
-        "value": round(pts / t_batched / 1e9, 4), "unit": "GPoint/s", "n_gpus": 1, "steps": nt,
+        "value": round(pts / t_batched / 1e9, 4), "unit": "GPoint/s", "n_gpus": world, "steps": nt,
         "warmup": 1, "ms_per_step": round(t_batched / nt * 1e3, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Gaussian-random-field velocities); no dataset involved",
         "config": {"workload": "batched multi-shot modelling, one CUDA graph", "shots": nshot,
-                   "sizes": [sizes[0], sizes[-1]], "order": order, "dx_m": dx, "sponge": 20},
+                   "sizes": [sizes[0], sizes[-1]], "order": order, "dx_m": dx, "sponge": 20,
+                   "parallelism": f"shots over {world} rank(s) by work, nothing exchanged"},
         "shots_per_s": round(nshot / t_batched, 4),
-        "plain": {"value": round(pts / t_plain / 1e9, 4), "unit": "GPoint/s",
-                  "form": "same kernels, one shot per launch, eager host loop, no CUDA graph "
-                          "(per-shot set-up not timed)",
-                  "seconds": round(t_plain, 3)},
-        "speedup_vs_plain": round(t_plain / t_batched, 3),
-        "traces_identical_to_plain": same,
-        "gpu_launches": launches,
+        "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": round(16 * pts / t_batched / 1e9, 1),
-                     "peak": peak, "unit": "GB/s",
-                     "frac": round(16 * pts / t_batched / 1e9 / peak, 4), "peak_source": peak_src},
+                     "peak": peak_job, "unit": "GB/s",
+                     "frac": round(16 * pts / t_batched / 1e9 / peak_job, 4),
+                     "peak_source": peak_src + (f" x {world} GPUs" if world > 1 else "")},
         "seconds": round(t_batched, 3),
     }
+    if plain is not None:
+        t_plain, same = plain
+        line["plain"] = {"value": round(pts / t_plain / 1e9, 4), "unit": "GPoint/s",
+                         "form": "same kernels, one shot per launch, eager host loop, no CUDA "
+                                 "graph (per-shot set-up not timed)",
+                         "seconds": round(t_plain, 3)}
+        line["speedup_vs_plain"] = round(t_plain / t_batched, 3)
+        line["traces_identical_to_plain"] = same
     print(json.dumps(line))
 
 
@@ -923,10 +1013,13 @@ def main():
                                   "numbers are in the b200 line; sustained: the reference CPU "
                                   "path of this step is the propa workload's reference line)"}))
             return
+        if a.workload in ("adjoint", "modeling"):
+            # shot-parallel: every rank runs its share of the survey
+            {"adjoint": adjoint_arm, "modeling": modeling_arm}[a.workload](a)
+            return
         if world > 1 and rank != 0:
             return
-        {"adjoint": adjoint_arm, "modeling": modeling_arm, "mixed": mixed_arm,
-         "fd": fd_arm, "sustained": sustained_arm}[a.workload](a)
+        {"mixed": mixed_arm, "fd": fd_arm, "sustained": sustained_arm}[a.workload](a)
         return
     if a.impl == "reference":
         reference_arm(a)

@@ -133,3 +133,42 @@ def test_batch_equals_single_shots_and_graph_equals_eager(gpu):
         assert gpu.equal(one.traces(0), both[i][0])
         assert gpu.equal(one.states[0].grad, both[i][1])
         one.close()
+
+
+def test_survey_gradient_is_the_sum_of_the_shards(gpu):
+    """The shot-parallel split: shots 0 and 2 on one 'rank', shot 1 on another, each its own
+    batch; the survey gradient (hpcscan_b200.shots) of the shards, summed, equals the per-shot
+    gradients of one batch of all three shots, summed in the same order (bit for bit: shots are
+    independent in a batch, and the sums are the same FP32 additions)."""
+    from hpcscan_b200.modeling import Batch
+    from hpcscan_b200.shots import my_shots, sum_gradients, survey_gradient
+    n = (30, 28, 26)
+    sizes = (n, n, n)
+    ref = Batch(make_shots(gpu, sizes, seed=3), ORDER, dt_of(), NT, F0)
+    ref.forward()
+    gpu.cuda.synchronize()
+    dobs = [ref.traces(i).clone() * 1.01 for i in range(3)]
+    ref.close()
+    full = Batch(make_shots(gpu, sizes, seed=3, dobs=dobs), ORDER, dt_of(), NT, F0, gradient=True,
+                 checkpoint=11)
+    full.forward()
+    full.backward()
+    gpu.cuda.synchronize()
+    per_shot = [full.gradient_of(i).clone() for i in range(3)]
+    assert gpu.equal(survey_gradient(full), (per_shot[0] + per_shot[1]) + per_shot[2])
+    full.close()
+    parts = [my_shots([1.0] * 3, r, 2) for r in range(2)]
+    assert parts == [[0, 2], [1]]
+    shots = make_shots(gpu, sizes, seed=3, dobs=dobs)
+    shard_sums = []
+    for part in parts:
+        b = Batch([shots[i] for i in part], ORDER, dt_of(), NT, F0, gradient=True, checkpoint=11)
+        b.forward()
+        b.backward()
+        gpu.cuda.synchronize()
+        for j, i in enumerate(part):
+            assert gpu.equal(b.gradient_of(j), per_shot[i])
+        shard_sums.append(survey_gradient(b))
+        b.close()
+    # the all-reduce of two ranks adds the two shard sums
+    assert gpu.equal(sum_gradients(shard_sums), (per_shot[0] + per_shot[2]) + per_shot[1])
