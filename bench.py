@@ -54,7 +54,9 @@ def parse_args():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
-    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"],
+                   help="b200 (this library), reference (the reference CPU path, the baseline) "
+                        "or reference-gpu (the reference's own CUDA modes on this GPU)")
     p.add_argument("--size", type=int, default=512)
     p.add_argument("--order", type=int, default=8)
     p.add_argument("--e2e-steps", type=int, default=0,
@@ -207,7 +209,7 @@ def run_reference_cpu(n: int, order: int, nt: int, threads: int):
     args = [exe, "-testCase", "Propa", "-testMode", "CacheBlk", "-propagator", "Ac2Standard",
             "-fdOrder", str(order), "-n1", str(n), "-n2", str(n), "-n3", str(n),
             "-ratioCFL", "0.8", "-param1", "1", "-param2", "1", "-param3", "1",
-            "-nt", str(nt), "-snapInc", str(nt), "-ntry", "1"]
+            "-nt", str(nt), "-snapInc", str(max(1, nt // 2)), "-ntry", "1"]
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
     with tempfile.TemporaryDirectory() as d:
         t0 = time.perf_counter()
@@ -225,7 +227,81 @@ def run_reference_cpu(n: int, order: int, nt: int, threads: int):
     pts = float(n) ** 3 * nt
     value = pts / (t_bc + t_p) / 1e9
     return value, {"bc_s": t_bc, "pressure_s": t_p, "gpoint_fd": grab(r"Best Gpoint/s in FD"),
-                   "wall_s": wall, "nt": nt}
+                   "wall_s": wall, "nt": nt, "passed": "Test PASSED" in txt,
+                   "err_test_case": grab(r"errTestCase2")}
+
+
+def run_reference_gpu(n: int, order: int, nt: int, mode: str, cb=None):
+    """Run the reference Propa test case in one of its own GPU test modes (CUDA, CUDA_Opt), built
+    unchanged from its sources for sm_100a, and return its own timers like run_reference_cpu.
+    cb: the reference's block sizes (-cb1, -cb2, -cb3), which size CUDA_Opt's tiles."""
+    from oracle import oracle
+    exe = oracle.ref_gpu_binary()
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    args = [exe, "-testCase", "Propa", "-testMode", mode, "-propagator", "Ac2Standard",
+            "-fdOrder", str(order), "-n1", str(n), "-n2", str(n), "-n3", str(n),
+            "-ratioCFL", "0.8", "-param1", "1", "-param2", "1", "-param3", "1",
+            "-nt", str(nt), "-snapInc", str(max(1, nt // 2)), "-ntry", "1"]
+    if cb is not None:
+        args += ["-cb1", str(cb[0]), "-cb2", str(cb[1]), "-cb3", str(cb[2])]
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        out = subprocess.run(args, cwd=d, capture_output=True, text=True, timeout=600)
+        wall = time.perf_counter() - t0
+    if out.returncode != 0:
+        raise RuntimeError((out.stdout[-1500:] + out.stderr[-1500:]).strip())
+    txt = out.stdout
+
+    def grab(pat):
+        m = re.search(pat + r"\s+(\S+)", txt)
+        return float(m.group(1)) if m else None
+    t_bc = grab(r"Bound\. cond\. time \(s\)")
+    t_p = grab(r"Compute pres\. time \(s\)")
+    if t_bc is None or t_p is None:
+        raise RuntimeError("no timers in the reference's output: " + txt[-800:])
+    return n ** 3 * nt / (t_bc + t_p) / 1e9, {
+        "mode": mode, "cb": cb, "bc_s": t_bc, "pressure_s": t_p,
+        "gpoint_fd": grab(r"Best Gpoint/s in FD"), "wall_s": round(wall, 2), "nt": nt,
+        "passed": "Test PASSED" in txt, "err_test_case": grab(r"errTestCase2")}
+
+
+def reference_gpu_arm(a):
+    """The reference's own GPU path on this GPU: its CUDA_Opt mode (2.5-D shared-memory tiles with
+    a register z-queue, one kernel per order) at its default block sizes and at two larger ones,
+    and its plain CUDA mode; the line reports the fastest, every run in `runs`. Not the driver's
+    reference arm (the reference CPU path, --impl reference): a comparison on the same GPU."""
+    rank, world, _ = dist_env()
+    if world > 1 and rank != 0:
+        return
+    nt = max(a.steps, 1)
+    runs, best = [], None
+    for mode, cb in (("CUDA_Opt", None), ("CUDA_Opt", (64, 16, 64)), ("CUDA_Opt", (64, 8, 32)),
+                     ("CUDA", None)):
+        try:
+            v, det = run_reference_gpu(a.size, a.order, nt, mode, cb)
+            runs.append({"value": round(v, 4), **det})
+            if best is None or v > best[0]:
+                best = (v, det)
+        except Exception as e:
+            runs.append({"mode": mode, "cb": cb, "failed": str(e)[:300]})
+    if best is None:
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "the reference's CUDA modes "
+                          "did not run", "runs": runs}))
+        return
+    v, det = best
+    print(json.dumps({
+        "impl": "reference-gpu", "metric": METRIC, "value": round(v, 4), "unit": UNIT,
+        "n_gpus": 1, "steps": nt, "warmup": 0,
+        "ms_per_step": round((det["bc_s"] + det["pressure_s"]) / nt * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (eigen mode, the reference's own Propa initialisation)",
+        "config": {"workload": f"Propa Ac2Standard O{a.order} FP32 {a.size}^3 eigen mode",
+                   "n": a.size, "order": a.order, "ratio_cfl": 0.8,
+                   "test_mode": f"{det['mode']} (reference GPU path, unchanged source, sm_100a)",
+                   "timers": "the reference's own boundary-condition + compute-pressure timers "
+                             "(each call ends with a device synchronisation)"},
+        "runs": runs}))
 
 
 def reference_arm(a):
@@ -1023,6 +1099,8 @@ def main():
         return
     if a.impl == "reference":
         reference_arm(a)
+    elif a.impl == "reference-gpu":
+        reference_gpu_arm(a)
     else:
         b200_arm(a)
 

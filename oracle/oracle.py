@@ -35,10 +35,18 @@ def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and, when the reference sources are present, the
     reference binaries in _ref/)."""
     targets = ["oracle"]
-    if os.path.isdir(os.environ.get("REF_SRC", "/root/reference/src")):
+    have_ref = os.path.isdir(os.environ.get("REF_SRC", "/root/reference/src"))
+    if have_ref:
         targets.append("ref")
     subprocess.run(["make", "-C", HERE, "-j8"] + targets, check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
+    if have_ref:
+        # the reference's own CUDA modes, a comparison point only: a failure here leaves the
+        # checker intact
+        r = subprocess.run(["make", "-C", HERE, "-j8", "ref-cuda"],
+                           stdout=subprocess.DEVNULL if quiet else None)
+        if r.returncode != 0:
+            print("oracle: the reference's CUDA modes did not build (comparison only)")
 
 
 _lib = None
@@ -252,6 +260,12 @@ def min_max(lay, u, box):
 def ref_binary(prec: str) -> str:
     """Path of the reference CPU binary built unchanged from the reference sources."""
     return os.path.join(REF_DIR, f"hpcscan_{'fp64' if prec == 'f64' else 'fp32'}")
+
+
+def ref_gpu_binary() -> str:
+    """Path of the reference built with its own CUDA test modes (CUDA, CUDA_Opt, CUDA_Ref), FP32,
+    unchanged sources, for sm_100a."""
+    return os.path.join(REF_DIR, "hpcscan_cuda_fp32")
 
 
 def eigen_fields(lay, setup, point_type_all=True):
