@@ -57,7 +57,8 @@ def parse_args():
     p.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"],
                    help="b200 (this library), reference (the reference CPU path, the baseline) "
                         "or reference-gpu (the reference's own CUDA modes on this GPU)")
-    p.add_argument("--size", type=int, default=512)
+    p.add_argument("--size", type=int, default=None,
+                   help="inner points per axis (default 512; the adjoint workload 256)")
     p.add_argument("--order", type=int, default=8)
     p.add_argument("--e2e-steps", type=int, default=0,
                    help="time steps of the end-to-end job (default: one period of the mode)")
@@ -73,7 +74,10 @@ def parse_args():
     p.add_argument("--shots", type=int, default=0, help="shots (adjoint: 16, modeling: 64)")
     p.add_argument("--nt", type=int, default=0, help="time steps (adjoint: 2000, modeling: 1500)")
     p.add_argument("--checkpoint", type=int, default=45, help="adjoint checkpoint interval")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.size is None:
+        a.size = 256 if a.workload == "adjoint" else 512
+    return a
 
 
 def dist_env():
@@ -616,7 +620,7 @@ def adjoint_arm(a):
     from hpcscan_b200.shots import my_shots, survey_gradient
 
     dist, rank, world, local = _shot_dist()
-    n = a.size if a.size != 512 else 256
+    n = a.size
     nshot = a.shots or 16
     if nshot < world:
         raise SystemExit(f"{nshot} shots for {world} ranks: every rank needs a shot")
