@@ -61,3 +61,23 @@ def test_missing_binary(monkeypatch, tmp_path):
     monkeypatch.setattr(oracle, "ref_gpu_binary", lambda: os.path.join(str(tmp_path), "absent"))
     with pytest.raises(FileNotFoundError):
         bench.run_reference_gpu(64, 8, 10, "CUDA", None)
+
+
+def test_reference_gpu_arm_reports_unavailable(monkeypatch, tmp_path, capsys):
+    import json
+    import types
+    monkeypatch.setattr(oracle, "ref_gpu_binary", lambda: os.path.join(str(tmp_path), "absent"))
+    bench.reference_gpu_arm(types.SimpleNamespace(steps=10, size=64, order=8))
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference-gpu" and "unavailable" in line
+    assert len(line["runs"]) == 4 and all("failed" in r for r in line["runs"])
+
+
+def test_reference_gpu_arm_picks_the_fastest(fake_ref, capsys):
+    import json
+    import types
+    bench.reference_gpu_arm(types.SimpleNamespace(steps=200, size=512, order=8))
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference-gpu" and line["metric"] == bench.METRIC
+    assert line["value"] == max(r["value"] for r in line["runs"])
+    assert line["config"]["test_mode"].startswith("CUDA_Opt")      # first of equal times
