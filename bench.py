@@ -20,7 +20,9 @@ device time is the max over ranks, and value = all points updated / that time.
                  against the measured HBM copy bandwidth
   cpu_baseline   the reference CPU path itself (oracle/_ref/hpcscan_fp32, test mode
                  CacheBlk, all host threads) on a bounded number of steps of the same grid
---impl reference prints the same line for the reference CPU implementation.
+--impl reference prints the same line for the reference CPU implementation; --impl
+reference-gpu for the reference's own CUDA modes (built unchanged for sm_100a) on this GPU, a
+comparison only.
 
 The other workloads (--workload) print their own line: adjoint and modeling split their
 fixed survey of shots over the ranks under torchrun (one GPU per rank, the adjoint's survey
