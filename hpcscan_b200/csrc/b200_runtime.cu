@@ -157,6 +157,12 @@ int check_box(const b200_layout* lay, const b200_box* b)
 		return set_error(B200_ERR_ARG, "box [%lld,%lld]x[%lld,%lld]x[%lld,%lld] outside the array",
 				(long long)b->i1s, (long long)b->i1e, (long long)b->i2s, (long long)b->i2e,
 				(long long)b->i3s, (long long)b->i3e);
+	// an end before its start would give negative extents, which the row walks would turn into
+	// indices past the box
+	if (b->i1e < b->i1s || b->i2e < b->i2s || b->i3e < b->i3s)
+		return set_error(B200_ERR_ARG, "box [%lld,%lld]x[%lld,%lld]x[%lld,%lld] has an end before its start",
+				(long long)b->i1s, (long long)b->i1e, (long long)b->i2s, (long long)b->i2e,
+				(long long)b->i3s, (long long)b->i3e);
 	return B200_OK;
 }
 

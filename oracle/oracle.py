@@ -31,20 +31,33 @@ class _Box(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("i1s", "i1e", "i2s", "i2e", "i3s", "i3e")]
 
 
+# where the build recipes look for the hpcscan sources when REF_SRC is not set: the read-only
+# checkout of the build container (absent on the GPU machines, which use the built files)
+_REF_CHECKOUT_SRC = "/root/reference/src"
+
+
+def reference_sources():
+    """The src/ directory of the hpcscan checkout the recipes compile from (REF_SRC, else the
+    build container's checkout), or None when neither exists."""
+    for d in (os.environ.get("REF_SRC"), _REF_CHECKOUT_SRC):
+        if d and os.path.isdir(d):
+            return os.path.abspath(d)
+    return None
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and, when the reference sources are present, the
     reference binaries in _ref/)."""
     targets = ["oracle"]
-    have_ref = os.path.isdir(os.environ.get("REF_SRC", "/root/reference/src"))
-    if have_ref:
+    ref_src = reference_sources()
+    if ref_src:
         targets.append("ref")
-    subprocess.run(["make", "-C", HERE, "-j8"] + targets, check=True,
-                   stdout=subprocess.DEVNULL if quiet else None)
-    if have_ref:
+    make = ["make", "-C", HERE, "-j8"] + ([f"REF_SRC={ref_src}"] if ref_src else [])
+    subprocess.run(make + targets, check=True, stdout=subprocess.DEVNULL if quiet else None)
+    if ref_src:
         # the reference's own CUDA modes, a comparison point only: a failure here leaves the
         # checker intact
-        r = subprocess.run(["make", "-C", HERE, "-j8", "ref-cuda"],
-                           stdout=subprocess.DEVNULL if quiet else None)
+        r = subprocess.run(make + ["ref-cuda"], stdout=subprocess.DEVNULL if quiet else None)
         if r.returncode != 0:
             print("oracle: the reference's CUDA modes did not build (comparison only)")
 

@@ -47,6 +47,29 @@ def test_errors_are_status_codes_not_exits():
     assert rc == -1 and "axis 1" in _lib.last_error()
 
 
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_box_with_end_before_start_is_an_argument_error(axis):
+    """A box inside the array whose end lies before its start is refused before any launch
+    (fills, norms and the no-allocation norm): negative extents would otherwise walk rows past
+    the box."""
+    lib = _lib.load()
+    lay = _lib.Layout(16, 16, 16, 4, 11, 4, 11, 4, 11, 3, 4)
+    ends = [[4, 11], [4, 11], [4, 11]]
+    ends[axis] = [9, 6]
+    box = _lib.Box(ends[0][0], ends[0][1], ends[1][0], ends[1][1], ends[2][0], ends[2][1])
+    u = _lib.Field(1, _lib.B200_F32, 1.0)         # never dereferenced: the box check comes first
+    rc = lib.b200_fill_const(ctypes.byref(lay), u, ctypes.byref(box), 1.0, None)
+    assert rc == -1 and "end before its start" in _lib.last_error()
+    out = ctypes.c_double()
+    rc = lib.b200_sum_abs(ctypes.byref(lay), u, ctypes.byref(box), ctypes.byref(out), None)
+    assert rc == -1 and "end before its start" in _lib.last_error()
+    tab = (ctypes.c_double * 16)()
+    rc = lib.b200_l1_sums_separable_noalloc(ctypes.byref(lay), u, ctypes.byref(box), tab, tab, tab,
+                                            1.0, _lib.B200_F32, ctypes.byref(out),
+                                            ctypes.byref(out), None)
+    assert rc == -1 and "end before its start" in _lib.last_error()
+
+
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "nope.so"))

@@ -72,3 +72,18 @@ def test_noalloc_rejects_boxes_beyond_its_scratch(gpu):
     with pytest.raises(_lib.B200Error) as e:
         _sums("b200_l1_sums_separable_noalloc", grid, _tables(lay, 6), 1.0)
     assert e.value.code == -3 and str(TABLE_MAX) in str(e.value)
+
+
+def test_noalloc_calls_leave_free_device_memory_unchanged(gpu):
+    """The property the entry point exists for: once its first call on the device has set it up,
+    further calls take no device memory. Only no-alloc calls run between the two readings."""
+    lay = L.b200_layout(3, 64, 48, 40, order=8, prec="f32")
+    grid, tabs = _grid(lay, 7), _tables(lay, 8)
+    first = _sums("b200_l1_sums_separable_noalloc", grid, tabs, 1.3)     # set-up call
+    gpu.cuda.synchronize()
+    free0, _ = gpu.cuda.mem_get_info()
+    for _ in range(5):
+        assert _sums("b200_l1_sums_separable_noalloc", grid, tabs, 1.3) == first
+    gpu.cuda.synchronize()
+    free1, _ = gpu.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
