@@ -914,9 +914,14 @@ template <class Cfg>
 int pick_nz_chunk(int ntiles, int nz, int requested)
 {
 	if (requested > 0) return requested < nz ? requested : nz;
-	int per_sm = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zmarch<Cfg>, Cfg::NT, Cfg::SMEM);
-	if (per_sm < 1) per_sm = 1;
+	// resident CTAs per SM of this configuration, asked once per process (the call costs
+	// microseconds, which a caller that synchronises after every launch would see)
+	static const int per_sm_cached = [] {
+		int v = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_zmarch<Cfg>, Cfg::NT, Cfg::SMEM);
+		return v;
+	}();
+	const int per_sm = per_sm_cached < 1 ? 1 : per_sm_cached;
 	const int resident = per_sm * num_sms();
 	int chunk = Cfg::R <= 2 ? 64 : 128;
 	while (chunk > 16 && (int64_t)ntiles * ((nz + chunk - 1) / chunk) < 2 * (int64_t)resident) chunk /= 2;

@@ -153,3 +153,40 @@ def test_modeling_b200_traces_equal_reference(tmp_path, prec, boundary):
     assert got.shape == want.shape and np.abs(want).max() > 0
     err = np.abs(got - want).max() / np.abs(want).max()
     assert err <= (1e-6 if prec == "fp32" else 1e-13), err
+
+
+# ---- the stated sizes of the benchmarked configurations ----------------------------------------
+
+@pytest.mark.gpu
+def test_propa_config_200_cubed_one_period_equals_reference(tmp_path):
+    """The plain Propa configuration at its stated size: Ac2Standard, O8, FP32, 200^3 inner
+    points of the unit cube, ratioCFL 0.8, one period of the (1, 1, 1) eigen mode (tmax =
+    2 / sqrt(3), 635 time steps), the analytic check every step. The B200 errTestCase equals the
+    reference CPU build's (the CacheBlk mode, the reference's optimised CPU path) within 1e-5
+    relative; both pass the reference's own 2e-2 bar (src/testCase_Propa.cpp:91)."""
+    args = ["-testCase", "Propa", "-propagator", "Ac2Standard", "-fdOrder", "8",
+            "-n1", "200", "-n2", "200", "-n3", "200", "-ratioCFL", "0.8", "-tmax", "1.1547005",
+            "-ntry", "1"]
+    out_b200 = run(B200_BIN["fp32"], args + ["-testMode", "B200"], tmp_path)
+    out_ref = run(REF_BIN["fp32"], args + ["-testMode", "CacheBlk"], tmp_path)
+    got, want = propa_err(out_b200), propa_err(out_ref)
+    for out in (out_b200, out_ref):
+        assert re.findall(r"No\. time steps\s+(\d+)", out)[-1] == "635", out[-3000:]
+    assert abs(got - want) <= 1e-5 * abs(want), (got, want)
+    assert 3.0e-4 < got < 4.5e-4, got          # the reference's 3.737e-4 at this configuration
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("order", [2, 4, 8, 12, 16])
+def test_fd_d2_sweep_128_cubed_equals_reference(tmp_path, prec, order):
+    """The FD_D2 sweep's smallest cube (128^3, u = sin(4 pi x1) sin(6 pi x2) sin(8 pi x3)) for
+    every order of the sweep: the same four L1 errors against the analytic derivatives and the
+    same verdicts as the reference CPU build (src/testCase_FD_D2.cpp:65-74)."""
+    args = ["-testCase", "FD_D2", "-fdOrder", str(order), "-n1", "128", "-n2", "128",
+            "-n3", "128", "-param1", "4", "-param2", "6", "-param3", "8", "-param4", "1",
+            "-ntry", "1"]
+    got = results(run(B200_BIN[prec], args + ["-testMode", "B200"], tmp_path))
+    want = results(run(REF_BIN[prec], args + ["-testMode", "CacheBlk"], tmp_path))
+    assert len(got) == 4
+    same_results(got, want, rtol=1e-5, atol=1e-12)
