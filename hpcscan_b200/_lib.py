@@ -102,6 +102,10 @@ SIGNATURES = {
     "b200_batch_adjoint_step": [_VP, _I, _I, _VP],
     "b200_batch_gradient": [_VP, _I, _I, _VP],
     "b200_batch_info": [_VP, ctypes.POINTER(_I)],
+    "b200_set_autotune": [_I],
+    "b200_get_autotune": [ctypes.POINTER(_I)],
+    "b200_get_tuned_config": [_PL, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                              ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "b200_set_arith_mode": [_I],
     "b200_get_arith_mode": [ctypes.POINTER(_I)],
     "b200_set_stencil_config": [_I, _I, _I, _I, _I],

@@ -7,6 +7,7 @@
 // fastest, which every later launch of that key uses (the reference's -cb1/-cb2/-cb3
 // cache-block sweep, src/grid_Cuda_Optim.cu:2163-2211 and script/testCase_FD_D2/
 // cacheBlkAnalysis, made automatic).
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -63,10 +64,24 @@ struct Tuned {
 	int nz_chunk = 0;   // 0: heuristic
 	bool fused = false; // MODE_STEP only: the fused kernel beat BC + pressure when tuned
 };
-using TuneKey = std::tuple<int, int, int, int>;   // dtype, R, mode, exact
-std::map<TuneKey, Tuned> g_tuned;
+// (dtype, R, mode, exact) and, for entries the autotuner measured, the grid's n1, n2, n3
+using TuneKey = std::tuple<int, int, int, int, int64_t, int64_t, int64_t>;
+std::map<TuneKey, Tuned> g_tuned;      // measured by the autotuner, per grid size
+std::map<TuneKey, Tuned> g_forced;     // set by b200_set_stencil_config (any grid size)
 std::mutex g_tune_mutex;
 int g_arith = B200_ARITH_EXACT;
+// tuning on first use: -1 = not decided yet (environment HPCSCAN_B200_AUTOTUNE, default on)
+int g_autotune = -1;
+std::mutex g_autotune_mutex;           // one first-use tuning at a time
+// grids smaller than this (inner points) keep the defaults: their launches are too short to
+// rank shapes reliably, and tuning them would cost more than it saves
+constexpr int64_t kAutotuneMinPoints = int64_t(1) << 24;
+
+TuneKey key_of(int dtype, int R, int mode, bool exact, const b200_layout* lay)
+{
+	return TuneKey{dtype, R, mode, exact ? 1 : 0, lay ? lay->n1 : 0, lay ? lay->n2 : 0,
+	               lay ? lay->n3 : 0};
+}
 
 // Untuned defaults: the fastest shape of the pressure update measured at 512^3 on B200 for each
 // storage type and half width, interleaved runs (FP32: the two-row 28x64 tiles up to R = 2, the
@@ -85,12 +100,36 @@ Tuned default_tuning(int dtype, int R)
 	return t;
 }
 
-Tuned tuned_for(int dtype, int R, int mode, bool exact)
+// The launch parameters of a key: an explicit setting, else what the autotuner measured for
+// this grid size, else the defaults. *measured tells whether a measured or explicit entry
+// exists (false: the defaults were returned).
+Tuned tuned_for(int dtype, int R, int mode, bool exact, const b200_layout* lay,
+		bool* measured = nullptr)
 {
 	std::lock_guard<std::mutex> lock(g_tune_mutex);
-	auto it = g_tuned.find(TuneKey{dtype, R, mode, exact ? 1 : 0});
-	if (it != g_tuned.end()) return it->second;
+	if (measured) *measured = true;
+	auto f = g_forced.find(key_of(dtype, R, mode, exact, nullptr));
+	if (f != g_forced.end()) return f->second;
+	if (lay) {
+		auto it = g_tuned.find(key_of(dtype, R, mode, exact, lay));
+		if (it != g_tuned.end()) return it->second;
+	}
+	if (measured) *measured = false;
 	return has_shapes(mode) ? default_tuning(dtype, R) : Tuned{};
+}
+
+// Times the candidates of one key on scratch grids and records the fastest (the body of
+// b200_autotune_stencil, defined below).
+int autotune_key(const b200_layout* lay, int order, int dtype, int op, int reps,
+		int* best_shape = nullptr, int* best_chunk = nullptr, double* best_ms = nullptr);
+
+bool autotune_enabled()
+{
+	if (g_autotune < 0) {
+		const char* e = std::getenv("HPCSCAN_B200_AUTOTUNE");
+		g_autotune = (e && e[0] == '0') ? B200_AUTOTUNE_OFF : B200_AUTOTUNE_ON;
+	}
+	return g_autotune == B200_AUTOTUNE_ON;
 }
 
 int launch(const ZLaunch& L)
@@ -178,7 +217,28 @@ int run_zmarch(int mode, const b200_layout* lay, int order, const b200_field& in
 		if (reinterpret_cast<uintptr_t>(coef->data) % 16) return B200_OK;
 	}
 	const bool exact = !has_shapes(mode) || g_arith == B200_ARITH_EXACT;
-	const Tuned t = tuned_for(in.dtype, order / 2, mode, exact);
+	bool measured = false;
+	Tuned t = tuned_for(in.dtype, order / 2, mode, exact, lay, &measured);
+	if (!measured && has_shapes(mode) && autotune_enabled()) {
+		// first use of this (grid size, storage type, order, operator): time the candidates once
+		// and keep the fastest for every later launch (not while the stream is being captured:
+		// the tuning allocates and synchronises)
+		const int64_t inner = (int64_t)(lay->e1 - lay->s1 + 1) * (lay->e2 - lay->s2 + 1) *
+		                      (lay->e3 - lay->s3 + 1);
+		cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+		cudaStreamIsCapturing(s, &cap);
+		if (inner >= kAutotuneMinPoints && cap == cudaStreamCaptureStatusNone) {
+			std::lock_guard<std::mutex> guard(g_autotune_mutex);
+			if (int rc = autotune_key(lay, order, in.dtype, mode, 5)) {
+				// could not tune (e.g. no device memory for the scratch grids): remember the
+				// defaults for this key so that the next launch does not try again
+				std::lock_guard<std::mutex> lock(g_tune_mutex);
+				g_tuned[key_of(in.dtype, order / 2, mode, exact, lay)] = t;
+				(void)rc;
+			}
+			t = tuned_for(in.dtype, order / 2, mode, exact, lay);
+		}
+	}
 	if (mode == MODE_STEP && !t.fused) return B200_OK;   // separate BC + pressure is faster
 	*handled = 1;
 	ZLaunch L;
@@ -232,13 +292,13 @@ int b200_set_stencil_config(int dtype, int order, int op, int shape, int nz_chun
 		return set_error(B200_ERR_ARG, "shape %d", shape);
 	if (nz_chunk < 0) return set_error(B200_ERR_ARG, "nz_chunk %d", nz_chunk);
 	std::lock_guard<std::mutex> lock(g_tune_mutex);
-	if (shape == -1) {   // back to the untuned defaults
-		for (int ex = 0; ex < 2; ex++) g_tuned.erase(TuneKey{dtype, order / 2, op, ex});
+	if (shape == -1) {   // back to the measured or default parameters
+		for (int ex = 0; ex < 2; ex++) g_forced.erase(key_of(dtype, order / 2, op, ex, nullptr));
 		return B200_OK;
 	}
 	// setting a shape for the fused step selects the fused kernel
 	for (int ex = 0; ex < 2; ex++)
-		g_tuned[TuneKey{dtype, order / 2, op, ex}] = Tuned{shape, nz_chunk, op == MODE_STEP};
+		g_forced[key_of(dtype, order / 2, op, ex, nullptr)] = Tuned{shape, nz_chunk, op == MODE_STEP};
 	return B200_OK;
 }
 
@@ -246,14 +306,57 @@ int b200_get_stencil_config(int dtype, int order, int op, int* shape, int* nz_ch
 {
 	if (!shape || !nz_chunk) return set_error(B200_ERR_ARG, "NULL output");
 	if (int rc = check_order(order)) return rc;
-	const Tuned t = tuned_for(dtype, order / 2, op, g_arith == B200_ARITH_EXACT || !has_shapes(op));
+	const Tuned t = tuned_for(dtype, order / 2, op, g_arith == B200_ARITH_EXACT || !has_shapes(op),
+			nullptr);
 	*shape = t.shape;
 	*nz_chunk = t.nz_chunk;
 	return B200_OK;
 }
 
+int b200_get_tuned_config(const b200_layout* lay, int order, int dtype, int op, int* shape,
+		int* nz_chunk, int* fused, int* measured)
+{
+	if (!shape || !nz_chunk || !fused || !measured) return set_error(B200_ERR_ARG, "NULL output");
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_order(order)) return rc;
+	bool m = false;
+	const Tuned t = tuned_for(dtype, order / 2, op, g_arith == B200_ARITH_EXACT || !has_shapes(op),
+			lay, &m);
+	*shape = t.shape;
+	*nz_chunk = t.nz_chunk;
+	*fused = t.fused ? 1 : 0;
+	*measured = m ? 1 : 0;
+	return B200_OK;
+}
+
+int b200_set_autotune(int mode)
+{
+	if (mode != B200_AUTOTUNE_OFF && mode != B200_AUTOTUNE_ON)
+		return set_error(B200_ERR_ARG, "autotune mode %d", mode);
+	g_autotune = mode;
+	return B200_OK;
+}
+
+int b200_get_autotune(int* mode)
+{
+	if (!mode) return set_error(B200_ERR_ARG, "mode is NULL");
+	*mode = autotune_enabled() ? B200_AUTOTUNE_ON : B200_AUTOTUNE_OFF;
+	return B200_OK;
+}
+
 int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, int reps,
 		int* best_shape, int* best_chunk, double* best_ms)
+{
+	return autotune_key(lay, order, dtype, op, reps, best_shape, best_chunk, best_ms);
+}
+
+}  // extern "C"
+
+namespace b200 {
+namespace {
+
+int autotune_key(const b200_layout* lay, int order, int dtype, int op, int reps, int* best_shape,
+		int* best_chunk, double* best_ms)
 {
 	if (int rc = check_layout(lay)) return rc;
 	if (int rc = check_order(order)) return rc;
@@ -262,11 +365,22 @@ int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, 
 		return set_error(B200_ERR_UNSUPPORTED, "layout/dtype not handled by the z-marching kernels");
 	if (op < MODE_D2_AXIS1 || op > MODE_STEP) return set_error(B200_ERR_ARG, "operator %d", op);
 	if (reps < 1) reps = 5;
+	if (op == MODE_STEP) {
+		// the fused step is compared with the boundary condition + the pressure kernel at its
+		// own best parameters for this grid: tune those first
+		bool have = false;
+		tuned_for(dtype, order / 2, MODE_PRESSURE, !has_shapes(MODE_PRESSURE) || g_arith == B200_ARITH_EXACT,
+				lay, &have);
+		if (!have)
+			if (int rc = autotune_key(lay, order, dtype, MODE_PRESSURE, reps)) return rc;
+	}
 	const size_t bytes = (size_t)npoint(lay) * dtype_size(dtype);
 	void* buf[3] = {nullptr, nullptr, nullptr};
 	int rc = B200_OK;
 	for (int i = 0; i < 3 && !rc; i++) {
-		rc = cuda_error(cudaMalloc(&buf[i], bytes), "cudaMalloc(autotune)");
+		const cudaError_t e = cudaMalloc(&buf[i], bytes);
+		if (e == cudaErrorMemoryAllocation) cudaGetLastError();   // not sticky: clear it
+		rc = cuda_error(e, "cudaMalloc(autotune)");
 		if (!rc) rc = cuda_error(cudaMemset(buf[i], 0, bytes), "cudaMemset(autotune)");
 	}
 	cudaStream_t s = nullptr;
@@ -318,7 +432,7 @@ int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, 
 		// the alternative: the boundary condition kernels + the best pressure kernel
 		ZLaunch P = L;
 		P.mode = MODE_PRESSURE;
-		const Tuned tp = tuned_for(dtype, order / 2, MODE_PRESSURE, L.exact);
+		const Tuned tp = tuned_for(dtype, order / 2, MODE_PRESSURE, L.exact, lay);
 		P.shape = tp.shape;
 		P.nz_chunk = tp.nz_chunk;
 		double sep = 1e300;
@@ -346,7 +460,7 @@ int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, 
 	if (rc) return rc;
 	{
 		std::lock_guard<std::mutex> lock(g_tune_mutex);
-		g_tuned[TuneKey{dtype, order / 2, op, L.exact ? 1 : 0}] = win;
+		g_tuned[key_of(dtype, order / 2, op, L.exact, lay)] = win;
 	}
 	if (best_shape) *best_shape = (op == MODE_STEP && !win.fused) ? -1 : win.shape;
 	if (best_chunk) *best_chunk = win.nz_chunk;
@@ -354,4 +468,5 @@ int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, 
 	return B200_OK;
 }
 
-}  // extern "C"
+}  // namespace
+}  // namespace b200

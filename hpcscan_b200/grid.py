@@ -50,6 +50,18 @@ def _stream_ptr(stream: Optional[torch.cuda.Stream]) -> ctypes.c_void_p:
     return ctypes.c_void_p(s.cuda_stream)
 
 
+def tuned_config(grid: "Grid", op: int) -> dict:
+    """Launch parameters the library uses for `op` on grids of this layout (b200_get_tuned_config):
+    tile shape, planes per CTA (0 = heuristic), fused step (op OP_STEP), measured or default."""
+    sh, ch, fu, me = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lay = grid.c_layout()
+    _lib.call("b200_get_tuned_config", ctypes.byref(lay), grid.layout.order,
+              _lib.DTYPE_CODE[grid.layout.prec], op, ctypes.byref(sh), ctypes.byref(ch),
+              ctypes.byref(fu), ctypes.byref(me))
+    return {"shape": sh.value, "nz_chunk": ch.value, "fused": bool(fu.value),
+            "measured": bool(me.value)}
+
+
 class Grid:
     """A grid of the B200 test mode: layout + device array (+ spacing/origin)."""
 
@@ -210,6 +222,19 @@ class Grid:
         lay = self.c_layout()
         _lib.call("b200_compute_pressure", ctypes.byref(lay), fdOrder, self.c_field(),
                   prc.c_field(), coef.c_field(), i1, i2, i3, _stream_ptr(stream))
+        return RTN_CODE_OK
+
+    def propagateStep(self, prc: "Grid", coef: "Grid", fdOrder: int,
+                      boundCondType: int = _lib.B200_BOUND_COND_ANTI_MIRROR, stream=None) -> int:
+        """prc.applyBoundaryCondition(boundCondType) then self.computePressureWithFD(prc, coef)
+        in one library call (b200_propagate_step)."""
+        if not self.sameSize(prc):
+            print_error("In Grid::computePressureWithFD, grids have not same size")
+            return RTN_CODE_KO
+        i1, i2, i3 = self.inv2()
+        lay = self.c_layout()
+        _lib.call("b200_propagate_step", ctypes.byref(lay), fdOrder, self.c_field(), prc.c_field(),
+                  coef.c_field(), i1, i2, i3, boundCondType, _stream_ptr(stream))
         return RTN_CODE_OK
 
     def applyBoundaryCondition(self, boundCondType: int = _lib.B200_BOUND_COND_ANTI_MIRROR,

@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .grid import Grid, init_device
+from .grid import Grid, init_device, tuned_config
 from .layout import ALL_POINTS, INNER_POINTS, GridLayout, b200_layout
 from .propa_setup import EIGEN_FUNCS, EigenSetup, eigen_setup, init_times
 
@@ -80,9 +80,25 @@ class Propagator_Ac2:
     # ---- time step -----------------------------------------------------------------------------
     def computeWavefieldNextTimeStep(self, prn: Grid, prc: Grid, stream=None) -> int:
         """halo exchange (none on one GPU) -> boundary condition -> FD kernel
-        (src/propagator_Ac2.cpp:366-395)."""
-        prc.applyBoundaryCondition(self.boundCondType, stream=stream)
-        return self.computePressureWithFD(prn, prc, stream=stream)
+        (src/propagator_Ac2.cpp:366-395), as one b200_propagate_step call: the library runs
+        the boundary-condition kernel and the pressure kernel, or, where the tuner measured it
+        faster for this grid, the pressure kernel with the boundary condition built inside its
+        tiles. prn and the inner points of prc are bit-identical either way (prc's halo points,
+        which no later read uses before the next boundary condition, are then left as they
+        were)."""
+        if not prn.sameSize(prc):
+            return self.computePressureWithFD(prn, prc, stream=stream)
+        return prn.propagateStep(prc, self.coefGrid, self.fdOrder, self.boundCondType,
+                                 stream=stream)
+
+    def step_config(self) -> dict:
+        """The launch parameters the library uses for this propagator's grids: the pressure
+        kernel's tile shape and planes per CTA, and whether the fused step was chosen
+        (measured = False: untuned defaults)."""
+        out = {}
+        for name, op in (("pressure", _lib.OP_PRESSURE), ("step", _lib.OP_STEP)):
+            out[name] = tuned_config(self.prnGrid, op)
+        return out
 
     def computePressureWithFD(self, prn: Grid, prc: Grid, stream=None) -> int:
         return prn.computePressureWithFD(prc, self.coefGrid, self.fdOrder, stream=stream)
@@ -98,6 +114,12 @@ class Propagator_Ac2SplitComp(Propagator_Ac2):
         self.laplaGrid = Grid(self.layout, self.setup.samp, self.device, scale=self.wave_scale)
         self.laplaGrid.initializeGrid()
         return rc
+
+    def computeWavefieldNextTimeStep(self, prn: Grid, prc: Grid, stream=None) -> int:
+        """boundary condition, then the Laplacian and the update (two operators, as the
+        reference's SplitComp propagator runs them)."""
+        prc.applyBoundaryCondition(self.boundCondType, stream=stream)
+        return self.computePressureWithFD(prn, prc, stream=stream)
 
     def computePressureWithFD(self, prn: Grid, prc: Grid, stream=None) -> int:
         prc.FD_LAPLACIAN(INNER_POINTS, self.laplaGrid, self.fdOrder, stream=stream)

@@ -303,6 +303,26 @@ int b200_get_stencil_config(int dtype, int order, int op, int* shape, int* nz_ch
 int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, int reps,
 		int* best_shape, int* best_chunk, double* best_ms);
 
+/* Tuning on first use (default on; the environment variable HPCSCAN_B200_AUTOTUNE=0 turns it
+ * off at start-up): the first launch of the Laplacian, pressure or fused-step kernel for a grid
+ * of at least 2^24 inner points runs b200_autotune_stencil for that grid size, storage type,
+ * order and operator (scratch grids of the layout's size are allocated and freed; the call
+ * synchronises) and every later launch of the key uses the result. Skipped while the stream
+ * is being captured, and for keys with an explicit b200_set_stencil_config. The choice of
+ * shape never changes results: every shape evaluates the same expressions in the same order.
+ * The role of the reference's -cb1/-cb2/-cb3 sweep (src/grid_Cuda_Optim.cu:2163-2211),
+ * automatic; no reference counterpart as an entry point. */
+#define B200_AUTOTUNE_OFF 0
+#define B200_AUTOTUNE_ON  1
+int b200_set_autotune(int mode);
+int b200_get_autotune(int* mode);
+
+/* The launch parameters a grid of this layout gets for (dtype, order, op): tile shape, planes
+ * per CTA (0 = heuristic), fused step chosen (op 6), and whether they come from a measurement
+ * or an explicit setting (*measured = 1) or from the defaults (0). No device work. */
+int b200_get_tuned_config(const b200_layout* lay, int order, int dtype, int op, int* shape,
+		int* nz_chunk, int* fused, int* measured);
+
 /* ---- diagnostics ----------------------------------------------------------------------------
  * Device-side error word of the library's kernels (0 = none; bit 0: a producer gave up a
  * bounded wait, bit 1: a consumer did). Synchronous; `clear` resets it. No reference
