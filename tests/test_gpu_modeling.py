@@ -212,3 +212,49 @@ def test_gpu_gradient_matches_central_differences(gpu):
     fd = (misfit(+1.0) - misfit(-1.0)) / 2.0
     assert an > 0.0
     assert fd == pytest.approx(an, rel=2e-2), (fd, an)
+
+
+def test_dot_product_of_the_gpu_forward_adjoint_pair(gpu):
+    """The GPU forward and adjoint kernels are each other's transpose: with d = F(amp s) the
+    traces of the forward pass and r a random residual injected by the adjoint pass,
+    <d, r> = <amp s, w_src> / C(src), w_src[n] = w[n+1](src) read after each adjoint step.
+    FP32 kernels, FP64 sums; two shots of different sizes in one batch."""
+    import ctypes
+
+    from hpcscan_b200 import _lib
+    from hpcscan_b200.modeling import Batch
+    b = Batch(make_shots(gpu), ORDER, dt_of(), NT, F0)
+    b.forward()
+    gpu.cuda.synchronize()
+    d = [b.traces(i).clone() for i in range(2)]
+    b.close()
+    rng = np.random.default_rng(11)
+    r = [torch_randn(gpu, x.shape, rng) for x in d]
+    # the adjoint pass alone, driven by the residual r: traces = r, dobs = 0
+    a = Batch(make_shots(gpu, dobs=[gpu.zeros_like(x) for x in d]), ORDER, dt_of(), NT, F0,
+              gradient=True, checkpoint=NT)
+    for i, st in enumerate(a.states):
+        st.traces.copy_(r[i])                                   # residual row k-1 = traces - dobs
+        a._zero(st.adj, None)
+    wsrc = [gpu.zeros(NT, dtype=gpu.float32, device="cuda:0") for _ in range(2)]
+    idx = [gpu.tensor([st.src_flat], dtype=gpu.int64, device="cuda:0") for st in a.states]
+    s = ctypes.c_void_p(gpu.cuda.current_stream().cuda_stream)
+    for k in range(NT, 0, -1):
+        scur = (NT - k) % 2
+        _lib.call("b200_batch_adjoint_step", a.handle, k, scur, s)
+        for i, st in enumerate(a.states):                       # w[k](src) -> w_src[k - 1]
+            f = _lib.Field(ctypes.c_void_p(st.adj[1 - scur].data_ptr()), _lib.B200_F32, 1.0)
+            _lib.call("b200_gather_points", f, ctypes.c_void_p(idx[i].data_ptr()), 1,
+                      ctypes.c_void_p(wsrc[i][k - 1:].data_ptr()), 1, s)
+    gpu.cuda.synchronize()
+    for i, st in enumerate(a.states):
+        lhs = float((d[i].double() * r[i].double()).sum())
+        csrc = float(st.coef[st.src_flat])
+        rhs = float((2.0 * st.wavelet.double() * wsrc[i].double()).sum()) / csrc
+        assert abs(lhs) > 0
+        assert rhs == pytest.approx(lhs, rel=1e-4), (i, lhs, rhs)
+    a.close()
+
+
+def torch_randn(torch, shape, rng):
+    return torch.from_numpy(rng.standard_normal(tuple(shape)).astype(np.float32)).to("cuda:0")
