@@ -318,6 +318,15 @@ def reference_gpu_arm(a):
         "runs": runs}))
 
 
+def propa_config(a, layout_n1, l2, tuning, parallelism):
+    """The config object of the Propa lines, the same keys for this library's arm and the
+    reference arm."""
+    return {"workload": f"Propa Ac2Standard O{a.order} FP32 {a.size}^3 eigen mode "
+                        "(boundary condition + pressure update per step)",
+            "n": a.size, "order": a.order, "ratio_cfl": 0.8, "layout_n1": layout_n1, "l2": l2,
+            "tuning": tuning, "parallelism": parallelism}
+
+
 def reference_arm(a):
     rank, world, _ = dist_env()
     if world > 1 and rank != 0:
@@ -335,9 +344,11 @@ def reference_arm(a):
         "ms_per_step": round((det["bc_s"] + det["pressure_s"]) / nt * 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (eigen mode, the reference's own Propa initialisation)",
-        "config": {"workload": f"Propa Ac2Standard O{a.order} FP32 {a.size}^3 eigen mode",
-                   "n": a.size, "order": a.order, "ratio_cfl": 0.8,
-                   "test_mode": "CacheBlk (reference CPU, unchanged source)"},
+        "config": propa_config(a, layout_n1=a.size + 2 * (a.order // 2),
+                               l2="inputs larger than L2 (the host's caches)",
+                               tuning="CacheBlk (reference CPU, unchanged source), its default "
+                                      "cache blocks",
+                               parallelism=f"OpenMP x{threads} host threads"),
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads,
                          "kind": "reference",
                          "sample": f"{nt} time steps of {a.size}^3, timed by the reference's own "
@@ -482,12 +493,10 @@ def b200_arm(a):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (eigen mode sin(pi x) sin(pi y) sin(pi z), the reference's Propa "
                 "initialisation; no dataset involved)",
-        "config": {"workload": f"Propa Ac2Standard O{a.order} FP32 {a.size}^3 eigen mode "
-                               "(BC + fused pressure update per step)",
-                   "n": a.size, "order": a.order, "ratio_cfl": 0.8, "layout_n1": lay.n1,
-                   "l2": "inputs larger than L2 (3 x %.0f MB grids vs 126 MB L2)" % (lay.nbytes / 1e6),
-                   "tuning": tuning,
-                   "parallelism": f"replicas x{world}"},
+        "config": propa_config(a, layout_n1=lay.n1,
+                               l2="inputs larger than L2 (3 x %.0f MB grids vs 126 MB L2)"
+                                  % (lay.nbytes / 1e6),
+                               tuning=tuning, parallelism=f"replicas x{world}"),
         # per step: the boundary condition (one launch when every axis has 2 halo + 2 inner
         # points, else halos + planes) and the pressure kernel
         "gpu_launches": (2 if (fused or min(lay.n_inner) >= 2 * lay.halo + 2) else 3) * a.steps,
