@@ -132,6 +132,18 @@ bool autotune_enabled()
 	return g_autotune == B200_AUTOTUNE_ON;
 }
 
+// HPCSCAN_B200_FUSED_STEP=1 in the environment: b200_propagate_step takes the fused kernel for
+// every grid it accepts, without measuring (the way to select it from a program that cannot
+// call b200_set_stencil_config, such as hpcscan's own drivers); read once.
+bool fused_step_forced()
+{
+	static const bool forced = [] {
+		const char* e = std::getenv("HPCSCAN_B200_FUSED_STEP");
+		return e && e[0] == '1';
+	}();
+	return forced;
+}
+
 int launch(const ZLaunch& L)
 {
 	switch (L.mode) {
@@ -219,7 +231,8 @@ int run_zmarch(int mode, const b200_layout* lay, int order, const b200_field& in
 	const bool exact = !has_shapes(mode) || g_arith == B200_ARITH_EXACT;
 	bool measured = false;
 	Tuned t = tuned_for(in.dtype, order / 2, mode, exact, lay, &measured);
-	if (!measured && has_shapes(mode) && autotune_enabled()) {
+	if (!measured && has_shapes(mode) && autotune_enabled() &&
+			!(mode == MODE_STEP && fused_step_forced())) {
 		// first use of this (grid size, storage type, order, operator): time the candidates once
 		// and keep the fastest for every later launch (not while the stream is being captured:
 		// the tuning allocates and synchronises)
@@ -239,6 +252,7 @@ int run_zmarch(int mode, const b200_layout* lay, int order, const b200_field& in
 			t = tuned_for(in.dtype, order / 2, mode, exact, lay);
 		}
 	}
+	if (mode == MODE_STEP && fused_step_forced()) t.fused = true;
 	if (mode == MODE_STEP && !t.fused) return B200_OK;   // separate BC + pressure is faster
 	*handled = 1;
 	ZLaunch L;

@@ -83,7 +83,8 @@ shared_ptr<hpcscan::DataAcquisition> CAT(__wrap_, ACQ_CREATE)(string testMode)
 }
 
 // Propagators whose MODELING set-up uploads the coef grid (Propagator_Factory::create,
-// src/propagator_Factory.cpp:19-40); the test mode is the configuration's.
+// src/propagator_Factory.cpp:19-40), and the fused-step propagator Ac2Fused; the test mode is
+// the configuration's.
 shared_ptr<hpcscan::Propagator_Ac2> CAT(__wrap_, PROPA_CREATE)(string propagator)
 {
 	if (hpcscan::Config::Instance()->testMode.compare(hpcscan::GRID_MODE_B200) == 0) {
@@ -91,6 +92,8 @@ shared_ptr<hpcscan::Propagator_Ac2> CAT(__wrap_, PROPA_CREATE)(string propagator
 			return std::make_shared<hpcscan::Propagator_Ac2_B200>();
 		if (propagator.compare(hpcscan::PROPA_TYPE_AC2SPLITCOMP) == 0)
 			return std::make_shared<hpcscan::Propagator_Ac2SplitComp_B200>();
+		if (propagator.compare(hpcscan::PROPA_TYPE_AC2FUSED) == 0)
+			return std::make_shared<hpcscan::Propagator_Ac2Fused_B200>();
 	}
 	return CAT(__real_, PROPA_CREATE)(propagator);
 }

@@ -145,13 +145,28 @@ void Grid_B200::info(void)
 
 //-------------------------------------------------------------------------------------------------------
 
-b200_field Grid_B200::field(void) const
+b200_field Grid_B200::rawField(void) const
 {
 	b200_field f;
 	f.data = d_grid;
 	f.dtype = kDtype;
 	f.scale = 1.0f;
 	return f;
+}
+
+b200_field Grid_B200::field(void) const
+{
+	applyPendingBoundaryCondition();
+	return rawField();
+}
+
+bool Grid_B200::applyPendingBoundaryCondition(void) const
+{
+	if (bc_pending == 0) return true;
+	const int mask = bc_pending;
+	bc_pending = 0;
+	return ok(b200_apply_boundary(&lay, rawField(), B200_BOUND_COND_ANTI_MIRROR, mask, nullptr),
+			"Grid_B200::applyBoundaryCondition");
 }
 
 b200_box Grid_B200::box(Point_type pointType) const
@@ -207,6 +222,7 @@ Rtn_code Grid_B200::inv1(Myfloat64 out[3]) const
 Rtn_code Grid_B200::copyGridDeviceToHost(Point_type pointType) const
 {
 	const b200_box b = box(pointType);
+	applyPendingBoundaryCondition();
 	if (!ok(b200_copy_box_d2h(&lay, sizeof(Myfloat), grid_3d, d_grid, &b, nullptr),
 				"Grid_B200::copyGridDeviceToHost"))
 		return RTN_CODE_KO;
@@ -217,6 +233,7 @@ Rtn_code Grid_B200::copyGridHostToDevice(Point_type pointType)
 {
 	if (pointType == ALL_POINTS) host_ahead = false;
 	const b200_box b = box(pointType);
+	applyPendingBoundaryCondition();
 	if (!ok(b200_copy_box_h2d(&lay, sizeof(Myfloat), d_grid, grid_3d, &b, nullptr),
 				"Grid_B200::copyGridHostToDevice"))
 		return RTN_CODE_KO;
@@ -474,10 +491,35 @@ Rtn_code Grid_B200::applyBoundaryCondition(BoundCond_type boundCondType)
 	for (int f = 0; f < 6; f++)
 		if (f / 2 < dim && getNeighbourProc(faces[f]) == MPI_PROC_NULL) mask |= 1 << f;
 	host_ahead = false;
+	if (bc_defer) {              // built by the next propagateStep, or applied before any other use
+		bc_pending = mask;
+		return RTN_CODE_OK;
+	}
 	if (!ok(b200_apply_boundary(&lay, field(), B200_BOUND_COND_ANTI_MIRROR, mask, nullptr),
 				"Grid_B200::applyBoundaryCondition"))
 		return RTN_CODE_KO;
 	return ok(b200_stream_sync(nullptr), "Grid_B200::applyBoundaryCondition") ? RTN_CODE_OK : RTN_CODE_KO;
+}
+
+Rtn_code Grid_B200::propagateStep(Grid& prcGridIn, Grid& coefGridIn, Myint fdOrder)
+{
+	printDebug(FULL_DEBUG, "In Grid_B200::propagateStep");
+	Grid_B200* prc = dynamic_cast<Grid_B200*>(&prcGridIn);
+	const Grid_B200* coef = peer(coefGridIn, "Grid_B200::propagateStep");
+	if (!prc || !coef || this->sameSize(prcGridIn) != true || prc->bc_pending != 0x3F || dim != DIM3)
+		return computePressureWithFD(prcGridIn, coefGridIn, fdOrder);
+	// every face of a single-rank 3-D grid: the library's step (the fused kernel where the
+	// tuner measured it faster, else the boundary-condition and pressure kernels)
+	prc->bc_pending = 0;
+	host_ahead = false;
+	prc->host_ahead = false;
+	Myfloat64 i2[3];
+	inv2(i2);
+	if (!ok(b200_propagate_step(&lay, fdOrder, field(), prc->rawField(), coef->field(), i2[0], i2[1],
+				    i2[2], B200_BOUND_COND_ANTI_MIRROR, nullptr),
+				"Grid_B200::propagateStep"))
+		return RTN_CODE_KO;
+	return ok(b200_stream_sync(nullptr), "Grid_B200::propagateStep") ? RTN_CODE_OK : RTN_CODE_KO;
 }
 
 //-------------------------------------------------------------------------------------------------------

@@ -74,8 +74,18 @@ public:
 			const Grid& laplaGrid);
 	virtual Rtn_code computePressureWithFD(Grid& prcGridIn, Grid& coefGridIn, Myint fdOrder);
 
-	// device side of the grid
+	// device side of the grid (applies a deferred boundary condition first)
 	b200_field field(void) const;
+
+	// Deferred boundary condition, for the fused propagator step (Propagator_Ac2Fused_B200):
+	// once deferral is on, applyBoundaryCondition(BOUND_COND_ANTI_MIRROR) only records its
+	// faces; the next propagateStep with this grid as prc builds the condition inside the
+	// pressure kernel's tiles, and any other use of the grid's device data applies it first.
+	void deferBoundaryCondition(bool on) { bc_defer = on; }
+	// computePressureWithFD(prc, coef) of this grid with prc's deferred boundary condition, in
+	// one library call (b200_propagate_step); without a deferred condition on prc it is
+	// computePressureWithFD
+	Rtn_code propagateStep(Grid& prcGridIn, Grid& coefGridIn, Myint fdOrder);
 	const b200_layout& layout(void) const { return lay; }
 	// copy one point type of the grid between host (grid_3d) and device
 	Rtn_code copyGridDeviceToHost(Point_type) const;
@@ -95,6 +105,10 @@ private:
 	void* d_grid = nullptr;
 	b200_layout lay{};
 	mutable bool host_ahead = false;
+	bool bc_defer = false;
+	mutable int bc_pending = 0;          // faces of a deferred boundary condition (0: none)
+	b200_field rawField(void) const;     // the device field as it is
+	bool applyPendingBoundaryCondition(void) const;
 	b200_box box(Point_type) const;
 	// the device field of another grid of this mode, or nullptr (message printed)
 	static const Grid_B200* peer(const Grid& g, const char* caller);

@@ -166,7 +166,10 @@ int b200_apply_boundary(const b200_layout* lay, b200_field u, int bc_type, int f
  * followed by a small kernel that writes the boundary planes' zeros into prc; prn and the inner
  * points of prc end up bit-identical to the two separate calls, and prc's halo points are left
  * as they were (the next boundary condition rebuilds them before any read). Otherwise it runs
- * the boundary-condition kernels and the pressure kernel back to back. */
+ * the boundary-condition kernels and the pressure kernel back to back. With tuning on first use
+ * (b200_set_autotune) the choice is measured for each grid size of at least 2^24 inner points;
+ * HPCSCAN_B200_FUSED_STEP=1 in the environment selects the fused kernel for every grid it
+ * accepts. */
 int b200_propagate_step(const b200_layout* lay, int order, b200_field prn, b200_field prc,
 		b200_field coef, double inv2_1, double inv2_2, double inv2_3, int bc_type, void* stream);
 

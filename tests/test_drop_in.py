@@ -86,6 +86,50 @@ def test_propa_b200_equals_reference(tmp_path, prec, order, propagator):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fused", ["1", "0"])
+@pytest.mark.parametrize("prec,order", [("fp32", 8), ("fp32", 16), ("fp64", 4)])
+def test_propa_fused_propagator_equals_reference(tmp_path, monkeypatch, fused, prec, order):
+    """-propagator Ac2Fused (registered for -testMode B200): the boundary condition deferred by
+    the grids and built inside the pressure kernel's tiles (HPCSCAN_B200_FUSED_STEP=1) or run as
+    its own kernel in the same library call (0); errTestCase equal to the reference CPU build's
+    Ac2Standard, the analytic check every step."""
+    monkeypatch.setenv("HPCSCAN_B200_FUSED_STEP", fused)
+    args = ["-testCase", "Propa", "-fdOrder", str(order), "-n1", "70", "-n2", "61", "-n3", "53",
+            "-ratioCFL", "0.8", "-nt", "60", "-ntry", "1"]
+    out = run(B200_BIN[prec], args + ["-testMode", "B200", "-propagator", "Ac2Fused"], tmp_path)
+    assert "Boundary condition fused" in out
+    got = propa_err(out)
+    want = propa_err(run(REF_BIN[prec], args + ["-testMode", "Baseline", "-propagator",
+                                                "Ac2Standard"], tmp_path))
+    assert abs(got - want) <= 1e-5 * abs(want), (got, want)
+
+
+@pytest.mark.gpu
+def test_modeling_fused_propagator_traces_equal_reference(tmp_path, monkeypatch):
+    """TestCase_Modeling with -propagator Ac2Fused on B200 (fused kernel forced): the traces of
+    the reference CPU build's Ac2Standard (FP32, 1e-6 relative)."""
+    import numpy as np
+    monkeypatch.setenv("HPCSCAN_B200_FUSED_STEP", "1")
+    n = (48, 40, 44)
+    rng = np.random.default_rng(8)
+    vel = (2000.0 + 400.0 * np.tanh(rng.standard_normal((n[2], n[1], n[0])))).astype(np.float32)
+    runs = {}
+    for mode, binary, propa in (("B200", B200_BIN["fp32"], "Ac2Fused"),
+                                ("Baseline", REF_BIN["fp32"], "Ac2Standard")):
+        d = tmp_path / mode
+        d.mkdir()
+        vel.tofile(d / "vp.bin")
+        args = ["-testCase", "Modeling", "-testMode", mode, "-propagator", propa,
+                "-n1", str(n[0]), "-n2", str(n[1]), "-n3", str(n[2]), "-modelVpFile", "vp.bin",
+                "-nt", "160", "-ntry", "1"]
+        run(binary, args, d)
+        runs[mode] = np.fromfile(d / "ModelingForwardPrn.trace.bin", dtype=np.float32)
+    got, want = runs["B200"], runs["Baseline"]
+    assert got.shape == want.shape and np.abs(want).max() > 0
+    assert np.abs(got - want).max() / np.abs(want).max() <= 1e-6
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
 @pytest.mark.parametrize("order", [2, 4, 6, 8, 10, 12, 14, 16])
 def test_fd_d2_b200_equals_reference(tmp_path, prec, order):
