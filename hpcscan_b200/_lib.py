@@ -101,6 +101,7 @@ SIGNATURES = {
     "b200_batch_forward_step": [_VP, _I, _I, _I, _I, _VP],
     "b200_batch_adjoint_step": [_VP, _I, _I, _VP],
     "b200_batch_gradient": [_VP, _I, _I, _VP],
+    "b200_batch_survey_gradient": [_VP, _I, _I, _I, _I, _I, _VP, _VP],
     "b200_batch_info": [_VP, ctypes.POINTER(_I)],
     "b200_set_autotune": [_I],
     "b200_get_autotune": [ctypes.POINTER(_I)],

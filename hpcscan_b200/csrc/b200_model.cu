@@ -14,6 +14,7 @@
 // adjoint wavefields in 2, and each call names the slots it reads and writes. No call allocates
 // or synchronises, so a whole schedule can be captured in a CUDA graph.
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "b200_zmarch.cuh"
@@ -72,6 +73,47 @@ __global__ void k_model_residual(const MShot* __restrict__ shots, int k, int slo
 
 constexpr int kRecThreads = 128;
 
+// Survey gradient of shots on one grid, one step, no stencil: the forward recursion gives
+// C Lap p[n] = (p[n+1] - G amp s[n] delta_src + G^2 p[n-1]) / G - 2 p[n], so
+//   grad += kscale sum_s w_s[n+1] (p_s[n+1] / G_s + G_s p_s[n-1] - 2 p_s[n] - amp_s s[n] delta_src)
+// with the shots summed in batch order (one thread per point of the inner box, rows (i2, i3)
+// over the blocks, i1 over the threads: coalesced).
+struct SurveyArgs {
+	int64_t n1, n12, field;
+	int s1, e1, s2, e2, s3, e3;
+	int n, snext, scur, sprev, sadj, nshot;
+	float kscale;
+	float* grad;
+};
+
+__global__ void __launch_bounds__(256) k_survey_gradient(const MShot* __restrict__ shots, SurveyArgs a)
+{
+	const int nx = a.e1 - a.s1 + 1, ny = a.e2 - a.s2 + 1, nz = a.e3 - a.s3 + 1;
+	const int64_t rows = (int64_t)ny * nz;
+	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+		const int z = (int)(row / ny), y = (int)(row - (int64_t)z * ny);
+		const int i2 = a.s2 + y, i3 = a.s3 + z;
+		const int64_t base = (int64_t)i3 * a.n12 + (int64_t)i2 * a.n1;
+		for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+			const int i1 = a.s1 + x;
+			const int64_t idx = base + i1;
+			float acc = 0.0f;
+			for (int s = 0; s < a.nshot; s++) {
+				const MShot& m = shots[s];
+				const float G = (m.g1[i1] * m.g2[i2]) * m.g3[i3];
+				const float* w = m.wave;
+				const float p1 = w[a.snext * a.field + idx];
+				const float p0 = w[a.scur * a.field + idx];
+				const float pm = w[a.sprev * a.field + idx];
+				float c = fmaf(G, pm, p1 / G) - 2.0f * p0;
+				if (idx == m.src) c -= m.amp * m.wavelet[a.n];
+				acc = fmaf(m.adj[a.sadj * a.field + idx], c, acc);
+			}
+			a.grad[idx] = fmaf(a.kscale, acc, a.grad[idx]);
+		}
+	}
+}
+
 // Stencil passes: R and the tile shape (the pressure update's FP32 default: shape 0 up to
 // R = 2, shape 1 beyond), FP32 with fused multiply-adds.
 template <int R>
@@ -92,6 +134,10 @@ struct b200_batch {
 	int ctas = 0;                   // CTAs of one stencil pass over the whole batch
 	int max_nrec = 0;
 	int smem[3] = {0, 0, 0};
+	bool interleave = false;        // every shot has the same tiling: CTAs tile-major, shot-minor
+	bool same_grid = false;         // every shot has the same layout (the survey gradient)
+	b200_layout lay0{};             // the first shot's layout
+	float kscale = 0.0f;            // -1 / dt^2
 	ZShot* d_fwd = nullptr;         // stencil tables: forward, adjoint, gradient
 	ZShot* d_adj = nullptr;
 	ZShot* d_grad = nullptr;
@@ -206,6 +252,11 @@ int batch_tables(b200_batch* b, const b200_shot* shots, double dt, std::vector<Z
 		}
 	}
 	b->ctas = cta;
+	b->interleave = true;
+	for (int i = 1; i < b->nshot; i++)
+		if (fwd[i].ntx != fwd[0].ntx || fwd[i].nty != fwd[0].nty || fwd[i].nzc != fwd[0].nzc ||
+				fwd[i].a.nz_chunk != fwd[0].a.nz_chunk)
+			b->interleave = false;
 	b->smem[0] = CF::SMEM;
 	b->smem[1] = CF::SMEM;
 	b->smem[2] = CG::SMEM;
@@ -217,7 +268,8 @@ int launch_pass(const b200_batch* b, const ZShot* table, int su, int sp0, int so
 		cudaStream_t s)
 {
 	using Cfg = ModelCfg<R, MODE>;
-	k_zmarch_batch<Cfg><<<b->ctas, Cfg::NT, Cfg::SMEM, s>>>(table, b->nshot, su, sp0, sout, step);
+	k_zmarch_batch<Cfg><<<b->ctas, Cfg::NT, Cfg::SMEM, s>>>(table, b->nshot, su, sp0, sout, step,
+			b->interleave ? 1 : 0);
 	return check_launch("k_zmarch_batch");
 }
 
@@ -280,6 +332,11 @@ int b200_batch_create(b200_batch** out, int order, int nslot, int nshot, const b
 	b->nslot = nslot;
 	b->has_adj = adj || grad;
 	b->has_grad = grad;
+	b->lay0 = shots[0].lay;
+	b->kscale = (float)(-1.0 / (dt * dt));
+	b->same_grid = true;
+	for (int i = 1; i < nshot; i++)
+		if (std::memcmp(&shots[i].lay, &shots[0].lay, sizeof(b200_layout)) != 0) b->same_grid = false;
 	std::vector<ZShot> fwd, ad, gr;
 	int rc = dispatch_order(order, [&](auto rt) {
 		constexpr int R = decltype(rt)::value;
@@ -369,6 +426,37 @@ int b200_batch_gradient(b200_batch* b, int swave, int sadj, void* stream)
 	if (swave < 0 || swave >= b->nslot || sadj < 0 || sadj > 1)
 		return set_error(B200_ERR_ARG, "gradient slots %d %d", swave, sadj);
 	return dispatch_pass(b, MODE_GRAD, b->d_grad, swave, sadj, 0, -1, as_stream(stream));
+}
+
+int b200_batch_survey_gradient(b200_batch* b, int n, int snext, int scur, int sprev, int sadj,
+		float* grad, void* stream)
+{
+	if (!b || !b->has_adj) return set_error(B200_ERR_ARG, "batch without adjoint wavefields");
+	if (!b->same_grid) return set_error(B200_ERR_UNSUPPORTED, "survey gradient: the shots are on different grids");
+	if (!grad || reinterpret_cast<uintptr_t>(grad) % 4) return set_error(B200_ERR_ARG, "grad");
+	for (int sl : {snext, scur, sprev})
+		if (sl < 0 || sl >= b->nslot) return set_error(B200_ERR_ARG, "survey gradient slot %d of %d", sl, b->nslot);
+	if (snext == scur || scur == sprev || snext == sprev)
+		return set_error(B200_ERR_ARG, "survey gradient slots must differ");
+	if (sadj < 0 || sadj > 1 || n < 0) return set_error(B200_ERR_ARG, "survey gradient step %d adjoint slot %d", n, sadj);
+	const b200_layout& l = b->lay0;
+	SurveyArgs a;
+	a.n1 = l.n1;
+	a.n12 = l.n1 * l.n2;
+	a.field = l.n1 * l.n2 * l.n3;
+	a.s1 = (int)l.s1; a.e1 = (int)l.e1;
+	a.s2 = (int)l.s2; a.e2 = (int)l.e2;
+	a.s3 = (int)l.s3; a.e3 = (int)l.e3;
+	a.n = n;
+	a.snext = snext; a.scur = scur; a.sprev = sprev; a.sadj = sadj;
+	a.nshot = b->nshot;
+	a.kscale = b->kscale;
+	a.grad = grad;
+	const int64_t rows = (int64_t)(l.e2 - l.s2 + 1) * (l.e3 - l.s3 + 1);
+	const int64_t cap = (int64_t)num_sms() * 8;
+	const int blocks = (int)(rows < cap ? rows : cap);
+	k_survey_gradient<<<blocks, 256, 0, as_stream(stream)>>>(b->d_m, a);
+	return check_launch("k_survey_gradient");
 }
 
 int b200_batch_info(const b200_batch* b, int* ctas_per_pass)

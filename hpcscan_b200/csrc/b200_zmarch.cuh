@@ -876,16 +876,24 @@ struct alignas(64) ZShot {
 	int cta_begin, ntx, nty, nzc;
 };
 
-// Every shot of a batch in one launch: CTA b works on the shot whose range holds b.
+// Every shot of a batch in one launch: CTA b works on the shot whose range holds b. With
+// `interleave` (every shot has the same tiling) CTA b works on shot b % nshot, tile b / nshot:
+// the CTAs of one tile of all shots run side by side, so that the tiles they share (the model of
+// shots on one grid) come from DRAM once and from L2 for the others.
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_zmarch_batch(const ZShot* __restrict__ shots,
-		int nshot, int slot_u, int slot_p0, int slot_out, int step)
+		int nshot, int slot_u, int slot_p0, int slot_out, int step, int interleave)
 {
 	const int b = (int)blockIdx.x;
-	int s = 0;
-	while (s + 1 < nshot && shots[s + 1].cta_begin <= b) ++s;
+	int s = 0, local = 0;
+	if (interleave) {
+		s = b % nshot;
+		local = b / nshot;
+	} else {
+		while (s + 1 < nshot && shots[s + 1].cta_begin <= b) ++s;
+		local = b - shots[s].cta_begin;
+	}
 	const ZShot& sh = shots[s];
-	const int local = b - sh.cta_begin;
 	const int bx = local % sh.ntx, by = (local / sh.ntx) % sh.nty, bz = local / (sh.ntx * sh.nty);
 	// the shot's arguments in shared memory: read far more often than the tensor maps
 	__shared__ ZArgs<float> args;

@@ -135,15 +135,28 @@ class Batch:
 
     `checkpoint` = k: the forward pass keeps (p[n-1], p[n]) every k steps and the backward pass
     recomputes each segment into a ring of k + 1 forward grids (memory per shot about
-    (2 nt / k + k + 5) grids)."""
+    (2 nt / k + k + 5) grids).
+
+    `survey` (shots on one grid size, gradient=True): the backward pass accumulates the survey
+    gradient (the sum over the shots) into one grid, one pass per step over all shots without a
+    stencil (b200_batch_survey_gradient: C Lap p[n] from p[n+1], p[n], p[n-1], which the segment
+    recompute keeps, one step further); the shots' own gradients are then not formed."""
 
     def __init__(self, shots: Sequence[Shot], order: int, dt: float, nt: int, f0: float,
-                 gradient: bool = False, checkpoint: int = 45, device: int = 0):
+                 gradient: bool = False, checkpoint: int = 45, device: int = 0,
+                 survey: bool = False):
         init_device(device)
         self.order, self.dt, self.nt, self.device = order, float(dt), int(nt), device
         self.gradient = gradient
+        self.survey = bool(survey)
+        if self.survey:
+            if not gradient:
+                raise ValueError("survey=True needs gradient=True")
+            if len({tuple(sh.n) for sh in shots}) != 1:
+                raise ValueError("survey=True needs every shot on the same grid size")
         self.k = max(1, min(int(checkpoint), self.nt)) if gradient else 1
-        self.nslot = self.k + 1 if gradient else 2
+        # the survey gradient reads p[n+1] at the segment's last step: one more slot
+        self.nslot = (self.k + 2 if self.survey else self.k + 1) if gradient else 2
         self.nckpt = (self.nt + self.k - 1) // self.k if gradient else 0
         dev = f"cuda:{device}"
         wav = torch.from_numpy(ricker(f0, dt, nt)).to(dev)
@@ -165,7 +178,8 @@ class Batch:
                 dobs=None if sh.dobs is None else sh.dobs.to(dev).float().contiguous(),
                 wave=torch.zeros((self.nslot, npt), dtype=torch.float32, device=dev),
                 adj=torch.zeros((2, npt), dtype=torch.float32, device=dev) if gradient else None,
-                grad=torch.zeros(npt, dtype=torch.float32, device=dev) if gradient else None,
+                grad=torch.zeros(npt, dtype=torch.float32, device=dev)
+                if gradient and not self.survey else None,
                 src_flat=int(_flat(lay, *sh.src)))
             if gradient:
                 if st.dobs is None:
@@ -190,8 +204,11 @@ class Batch:
             c.adj = st.adj.data_ptr() if st.adj is not None else None
             c.grad = st.grad.data_ptr() if st.grad is not None else None
         self._c_shots = c_shots
+        self.survey_grad = torch.zeros(self.states[0].lay.npoint, dtype=torch.float32,
+                                       device=dev) if self.survey else None
         self.handle = ctypes.c_void_p()
-        flags = (_lib.B200_BATCH_ADJOINT | _lib.B200_BATCH_GRADIENT) if gradient else 0
+        flags = ((_lib.B200_BATCH_ADJOINT if self.survey else
+                  _lib.B200_BATCH_ADJOINT | _lib.B200_BATCH_GRADIENT) if gradient else 0)
         _lib.call("b200_batch_create", ctypes.byref(self.handle), order, self.nslot, len(shots),
                   c_shots, self.dt, flags)
         n = ctypes.c_int()
@@ -244,6 +261,8 @@ class Batch:
     def backward(self, stream=None) -> None:
         """Adjoint and gradient of every shot, segment by segment from the checkpoints."""
         assert self.gradient
+        if self.survey:
+            return self._backward_survey(stream)
         for st in self.states:
             self._zero(st.adj, stream)
             self._zero(st.grad, stream)
@@ -263,13 +282,46 @@ class Batch:
                 _lib.call("b200_batch_gradient", self.handle, k - n0, 1 - scur, self._s(stream))
                 self.launches += 3
 
+    def _backward_survey(self, stream) -> None:
+        """backward() with the survey gradient: the segment's recompute runs one step further
+        (slot j holds p[n0 - 1 + j], j = 0 .. end - n0 + 1), and after adjoint step k the survey
+        pass adds w[k] (C Lap p[k - 1]) of every shot."""
+        for st in self.states:
+            self._zero(st.adj, stream)
+        self._zero(self.survey_grad, stream)
+        gptr = ctypes.c_void_p(self.survey_grad.data_ptr())
+        for c in range(self.nckpt - 1, -1, -1):
+            n0 = c * self.k
+            end = min(n0 + self.k, self.nt)
+            for st in self.states:
+                self._copy(st.wave[0], st.ckpt[c, 0], stream)
+                self._copy(st.wave[1], st.ckpt[c, 1], stream)
+            for n in range(n0, end):
+                j = n - n0 + 1
+                self._fwd(n, j, j - 1, j + 1, stream)
+            for k in range(end, n0, -1):
+                scur = (self.nt - k) % 2             # slot of w[k+1]
+                _lib.call("b200_batch_adjoint_step", self.handle, k, scur, self._s(stream))
+                j = k - n0                           # slot of p[k - 1]
+                _lib.call("b200_batch_survey_gradient", self.handle, k - 1, j + 1, j, j - 1,
+                          1 - scur, gptr, self._s(stream))
+                self.launches += 3
+
     # ---- results --------------------------------------------------------------------------------
     def traces(self, i: int) -> torch.Tensor:
         return self.states[i].traces
 
     def gradient_of(self, i: int) -> torch.Tensor:
         """dJ/dm of shot i on its inner points, (n3, n2, n1)."""
+        if self.survey:
+            raise ValueError("a survey batch forms the sum over its shots only (survey_gradient_of)")
         return inner_of(self.states[i].lay, self.states[i].grad)
+
+    def survey_gradient_of(self) -> torch.Tensor:
+        """The sum over the shots of dJ/dm on the common inner points (survey batches)."""
+        if not self.survey:
+            raise ValueError("not a survey batch")
+        return inner_of(self.states[0].lay, self.survey_grad)
 
     def misfit(self, i: int) -> float:
         st = self.states[i]

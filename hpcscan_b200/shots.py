@@ -77,5 +77,8 @@ def sum_gradients(grads: Sequence[torch.Tensor], group=None,
 
 def survey_gradient(batch, group=None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
     """sum_gradients over every shot of a gradient `Batch` (modeling.Batch with gradient=True),
-    on the shots' common inner grid (n3, n2, n1)."""
+    on the shots' common inner grid (n3, n2, n1); a survey batch (survey=True) already holds
+    that sum, which is then all-reduced."""
+    if getattr(batch, "survey", False):
+        return sum_gradients([batch.survey_gradient_of()], group, out)
     return sum_gradients([batch.gradient_of(i) for i in range(len(batch.states))], group, out)

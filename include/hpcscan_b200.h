@@ -265,6 +265,17 @@ int b200_batch_forward_step(b200_batch* batch, int n, int scur, int sprev, int s
 int b200_batch_adjoint_step(b200_batch* batch, int k, int scur, void* stream);
 /* grad += -(C/dt^2) adj[sadj] Lap wave[swave] for every shot. */
 int b200_batch_gradient(b200_batch* batch, int swave, int sadj, void* stream);
+/* The survey gradient of a batch whose shots share one grid layout, one step, for all shots in
+ * one pass without a stencil: the forward recursion gives C Lap p[n] = (p[n+1] - G amp s[n]
+ * delta_src + G^2 p[n-1]) / G - 2 p[n], so
+ *   grad += -(1/dt^2) sum_s w_s[n+1] (p_s[n+1] / G + G p_s[n-1] - 2 p_s[n] - amp s[n] delta_src)
+ * with wave[snext] = p[n+1], wave[scur] = p[n], wave[sprev] = p[n-1] and adj[sadj] = w[n+1] of
+ * every shot; `grad` is one grid of the common layout (device). The sum over the shots of their
+ * b200_batch_gradient contributions, up to FP32 rounding, at 16 bytes read per shot and point
+ * plus the gradient's read and write, where b200_batch_gradient reads 20 per shot. No
+ * counterpart in the reference. */
+int b200_batch_survey_gradient(b200_batch* batch, int n, int snext, int scur, int sprev, int sadj,
+		float* grad, void* stream);
 /* CTAs of one stencil pass over the whole batch. */
 int b200_batch_info(const b200_batch* batch, int* ctas_per_pass);
 

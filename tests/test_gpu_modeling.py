@@ -258,3 +258,41 @@ def test_dot_product_of_the_gpu_forward_adjoint_pair(gpu):
 
 def torch_randn(torch, shape, rng):
     return torch.from_numpy(rng.standard_normal(tuple(shape)).astype(np.float32)).to("cuda:0")
+
+
+def test_survey_gradient_equals_sum_of_shot_gradients(gpu):
+    """Shots on one grid (survey=True): the survey gradient accumulated in one stencil-free pass
+    per step (C Lap p[n] from p[n+1], p[n], p[n-1] by the forward recursion) equals the sum of
+    the per-shot gradients (stencil pass per shot) to FP32 rounding, matches the FP64 oracle's
+    summed gradients, and is bit-identical across checkpoint intervals."""
+    from hpcscan_b200.modeling import Batch
+    from hpcscan_b200.shots import survey_gradient
+    from oracle import oracle
+    sizes = ((36, 30, 40), (36, 30, 40), (36, 30, 40))
+    dobs = observed(gpu, sizes)
+    shots = lambda: make_shots(gpu, sizes, dobs=dobs)                              # noqa: E731
+    ref = Batch(shots(), ORDER, dt_of(), NT, F0, gradient=True, checkpoint=7)
+    ref.forward()
+    ref.backward()
+    want = survey_gradient(ref).double()
+    oracle_sum = None
+    for i in range(len(sizes)):
+        lay, C, G, src, rec, inv2, wav = oracle_inputs(ref, i)
+        _, g = oracle.model_gradient(lay, C, G, src, 2.0, wav, rec, inv2,
+                                     dobs[i].double().cpu().numpy(), ref.dt)
+        g = np.asarray(g).reshape(lay.n3, lay.n2, lay.n1)[
+            lay.a3.inner_start:lay.a3.inner_end + 1, lay.a2.inner_start:lay.a2.inner_end + 1,
+            lay.a1.inner_start:lay.a1.inner_end + 1]
+        oracle_sum = g if oracle_sum is None else oracle_sum + g
+    ref.close()
+    got = {}
+    for k in (7, 50):
+        b = Batch(shots(), ORDER, dt_of(), NT, F0, gradient=True, checkpoint=k, survey=True)
+        b.forward()
+        b.backward()
+        got[k] = survey_gradient(b).clone()
+        b.close()
+    assert gpu.equal(got[7], got[50])
+    g = got[7].double()
+    assert rel(g.cpu().numpy(), want.cpu().numpy()) < 1e-4, rel(g.cpu().numpy(), want.cpu().numpy())
+    assert rel(g.cpu().numpy(), oracle_sum) < 1e-3, rel(g.cpu().numpy(), oracle_sum)
