@@ -76,40 +76,65 @@ constexpr int kRecThreads = 128;
 // Survey gradient of shots on one grid, one step, no stencil: the forward recursion gives
 // C Lap p[n] = (p[n+1] - G amp s[n] delta_src + G^2 p[n-1]) / G - 2 p[n], so
 //   grad += kscale sum_s w_s[n+1] (p_s[n+1] / G_s + G_s p_s[n-1] - 2 p_s[n] - amp_s s[n] delta_src)
-// with the shots summed in batch order (one thread per point of the inner box, rows (i2, i3)
-// over the blocks, i1 over the threads: coalesced).
+// with the shots summed in batch order. One thread per 16-byte vector of four i1 points of a
+// row (rows start 16-byte aligned; the vector of the first inner point may begin in the halo,
+// whose lanes are read and written back unchanged), the shots' pointers staged in shared memory.
 struct SurveyArgs {
 	int64_t n1, n12, field;
+	int x0, nvx;                // first vector's i1 (multiple of 4), vectors per row
 	int s1, e1, s2, e2, s3, e3;
 	int n, snext, scur, sprev, sadj, nshot;
 	float kscale;
 	float* grad;
 };
+constexpr int kSurveyMaxShots = 64;      // shots staged per pass over the table
 
 __global__ void __launch_bounds__(256) k_survey_gradient(const MShot* __restrict__ shots, SurveyArgs a)
 {
-	const int nx = a.e1 - a.s1 + 1, ny = a.e2 - a.s2 + 1, nz = a.e3 - a.s3 + 1;
-	const int64_t rows = (int64_t)ny * nz;
-	for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
-		const int z = (int)(row / ny), y = (int)(row - (int64_t)z * ny);
-		const int i2 = a.s2 + y, i3 = a.s3 + z;
-		const int64_t base = (int64_t)i3 * a.n12 + (int64_t)i2 * a.n1;
-		for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-			const int i1 = a.s1 + x;
-			const int64_t idx = base + i1;
-			float acc = 0.0f;
-			for (int s = 0; s < a.nshot; s++) {
-				const MShot& m = shots[s];
-				const float G = (m.g1[i1] * m.g2[i2]) * m.g3[i3];
-				const float* w = m.wave;
-				const float p1 = w[a.snext * a.field + idx];
-				const float p0 = w[a.scur * a.field + idx];
-				const float pm = w[a.sprev * a.field + idx];
-				float c = fmaf(G, pm, p1 / G) - 2.0f * p0;
-				if (idx == m.src) c -= m.amp * m.wavelet[a.n];
-				acc = fmaf(m.adj[a.sadj * a.field + idx], c, acc);
+	__shared__ MShot sh[kSurveyMaxShots];
+	const int ny = a.e2 - a.s2 + 1, nz = a.e3 - a.s3 + 1;
+	const int64_t items = (int64_t)ny * nz * a.nvx;
+	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+	for (int base = 0; base < a.nshot; base += kSurveyMaxShots) {
+		const int ns = min(kSurveyMaxShots, a.nshot - base);
+		__syncthreads();
+		for (int i = threadIdx.x; i < ns; i += blockDim.x) sh[i] = shots[base + i];
+		__syncthreads();
+		for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < items; t += stride) {
+			const int64_t row = t / a.nvx;
+			const int xv = (int)(t - row * a.nvx);
+			const int z = (int)(row / ny), y = (int)(row - (int64_t)z * ny);
+			const int i1 = a.x0 + 4 * xv, i2 = a.s2 + y, i3 = a.s3 + z;
+			const int64_t idx = (int64_t)i3 * a.n12 + (int64_t)i2 * a.n1 + i1;
+			float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+			for (int s = 0; s < ns; s++) {
+				const MShot& m = sh[s];
+				const float g23 = m.g2[i2] * m.g3[i3];
+				const float4 g1 = *reinterpret_cast<const float4*>(m.g1 + i1);
+				const float4 p1 = *reinterpret_cast<const float4*>(m.wave + a.snext * a.field + idx);
+				const float4 p0 = *reinterpret_cast<const float4*>(m.wave + a.scur * a.field + idx);
+				const float4 pm = *reinterpret_cast<const float4*>(m.wave + a.sprev * a.field + idx);
+				const float4 w = *reinterpret_cast<const float4*>(m.adj + a.sadj * a.field + idx);
+				const float G[4] = {g1.x * g23, g1.y * g23, g1.z * g23, g1.w * g23};
+				const float P1[4] = {p1.x, p1.y, p1.z, p1.w}, P0[4] = {p0.x, p0.y, p0.z, p0.w};
+				const float PM[4] = {pm.x, pm.y, pm.z, pm.w}, W[4] = {w.x, w.y, w.z, w.w};
+				float* A = &acc.x;
+#pragma unroll
+				for (int e = 0; e < 4; e++) {
+					if (G[e] == 0.0f) continue;            // halo lanes: G = 0 there
+					float c = fmaf(G[e], PM[e], P1[e] / G[e]) - 2.0f * P0[e];
+					if (idx + e == m.src) c -= m.amp * m.wavelet[a.n];
+					A[e] = fmaf(W[e], c, A[e]);
+				}
 			}
-			a.grad[idx] = fmaf(a.kscale, acc, a.grad[idx]);
+			float4* gp = reinterpret_cast<float4*>(a.grad + idx);
+			float4 g = *gp;
+			float* G4 = &g.x;
+			const float* A = &acc.x;
+#pragma unroll
+			for (int e = 0; e < 4; e++)
+				if (i1 + e >= a.s1 && i1 + e <= a.e1) G4[e] = fmaf(a.kscale, A[e], G4[e]);
+			*gp = g;
 		}
 	}
 }
@@ -447,14 +472,20 @@ int b200_batch_survey_gradient(b200_batch* b, int n, int snext, int scur, int sp
 	a.s1 = (int)l.s1; a.e1 = (int)l.e1;
 	a.s2 = (int)l.s2; a.e2 = (int)l.e2;
 	a.s3 = (int)l.s3; a.e3 = (int)l.e3;
+	a.x0 = a.s1 / 4 * 4;
+	a.nvx = (a.e1 - a.x0) / 4 + 1;
 	a.n = n;
 	a.snext = snext; a.scur = scur; a.sprev = sprev; a.sadj = sadj;
 	a.nshot = b->nshot;
 	a.kscale = b->kscale;
 	a.grad = grad;
-	const int64_t rows = (int64_t)(l.e2 - l.s2 + 1) * (l.e3 - l.s3 + 1);
+	if ((l.n1 % 4) != 0) return set_error(B200_ERR_ARG, "survey gradient: n1 not a multiple of 4");
+	// the vectors of a row must stay inside it: the last one ends at most at n1 - 1
+	if (a.x0 + 4 * a.nvx > l.n1) return set_error(B200_ERR_ARG, "survey gradient: row vectors");
+	const int64_t items = (int64_t)(l.e2 - l.s2 + 1) * (l.e3 - l.s3 + 1) * a.nvx;
 	const int64_t cap = (int64_t)num_sms() * 8;
-	const int blocks = (int)(rows < cap ? rows : cap);
+	const int64_t want = (items + 255) / 256;
+	const int blocks = (int)(want < cap ? want : cap);
 	k_survey_gradient<<<blocks, 256, 0, as_stream(stream)>>>(b->d_m, a);
 	return check_launch("k_survey_gradient");
 }

@@ -551,6 +551,10 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 		}
 	}
 
+	// this thread's first point of output plane z0 (advanced by one plane per output plane; the
+	// stores check their bounds)
+	S* orow = static_cast<S*>(a.out) + X + (int64_t)Y0 * a.n1 + (int64_t)z0 * a.n12;
+	if constexpr (SLOTS) orow += slot_out * a.out_slot_stride;
 	// The loop runs UQ planes per pass, the pushes of a pass going to q[2 RZ + u] and the
 	// queue shifted by UQ once per pass: logical q[i] of sub-step u is q[u + i].
 	for (int jb = 0; jb < J; jb += UQ) {
@@ -559,7 +563,13 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 		const int j = jb + u;
 		if (j >= J) return;
 			const int s = ru.slot;
-			if (alive && !__all_sync(FULL, mbar_wait(&full_u[s], ru.phase, deadline))) alive = false;
+			if constexpr (Cfg::BC) {
+				// the fused boundary condition's named barriers need the lanes of a warp to agree
+				if (alive && !__all_sync(FULL, mbar_wait(&full_u[s], ru.phase, deadline))) alive = false;
+			} else {
+				// lanes give up on their own (each then skips its work; no barrier follows)
+				if (alive && !mbar_wait(&full_u[s], ru.phase, deadline)) alive = false;
+			}
 			if constexpr (Cfg::ZQ) {
 				if (alive) {
 					const S* t = su + s * UE;
@@ -810,8 +820,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 						}
 						const int Y = Y0 + v;
 						if (Y <= a.e2) {
-							S* dst = static_cast<S*>(a.out) + X + (int64_t)Y * a.n1 + (int64_t)k * a.n12;
-							if constexpr (SLOTS) dst += slot_out * a.out_slot_stride;
+							S* dst = orow + v * a.n1;
 							if (X >= a.s1 && X + VX - 1 <= a.e1) {
 								using Vec = std::conditional_t<VX * sizeof(S) == 16, uint4, uint2>;
 								Vec pk;
@@ -832,6 +841,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 				if constexpr (Cfg::P) mbar_arrive(&empty_p[rp.slot]);
 				rc.advance();
 				rp.advance();
+				orow += a.n12;
 			}
 			if constexpr (Cfg::ZQ && !Cfg::ZONLY) {
 				if (j < RZ || j >= J - RZ)     // planes that are never a centre plane
@@ -989,8 +999,13 @@ int launch_zmarch(const ZLaunch& L)
 // (VY = 2) pay off for R <= 2 only: from R = 3 on, the longer z queue makes the registers,
 // not the shared-memory traffic, the limit (measured on B200).
 template <typename S, int R, int SHAPE> struct Shape;
+// Shape 0 keeps FP32 R = 5..7 at two CTAs per SM (128 registers; one CTA of 8 warps at the
+// 170-200 registers these would take otherwise leaves the schedulers short of warps: at 512^3 on
+// B200 the pressure update takes 0.51 against 0.64 ms at O10, 0.58 against 0.66 at O12, 0.59
+// against 0.62 at O14, bit-identical; at O16 the spills make it slower).
 template <typename S, int R> struct Shape<S, R, 0> {
-	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 2, MINB = 0; };
+	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 2,
+	                     MINB = (sizeof(S) == 4 && R >= 5 && R <= 7) ? 2 : 0; };
 template <typename S, int R> struct Shape<S, R, 1> {   // shape 0 with a deeper prefetch ring
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 4, MINB = 0; };
 template <typename S, int R> struct Shape<S, R, 2> {   // 9 warps; two CTAs per SM for R <= 4
@@ -1003,7 +1018,14 @@ template <typename S, int R, int MODE, int SHAPE, bool EXACT>
 int launch_shape(const ZLaunch& L)
 {
 	using Sh = Shape<S, R, SHAPE>;
-	using Cfg = ZCfg<S, R, MODE, Sh::TX, Sh::TY, Sh::VY, Sh::PF, EXACT, Sh::MINB>;
+	// The y-only operators from R = 5 on: four rows per thread in 56-row tiles, so that the
+	// 2R + 4 rows a thread reads from shared memory serve four output rows (no z queue holds
+	// registers there): 0.22 against 0.32 ms for FD_D2_N2 O16 FP32 at 512^3 on B200 (at O8 the
+	// one-row tiles are as fast).
+	constexpr bool YROWS = (MODE == MODE_D2_AXIS2 || MODE == MODE_D1_AXIS2) && R >= 5;
+	// the fused step keeps its registers (its in-tile boundary condition spills at 128)
+	using Cfg = ZCfg<S, R, MODE, Sh::TX, YROWS ? 56 : Sh::TY, YROWS ? 4 : Sh::VY, Sh::PF, EXACT,
+			MODE == MODE_STEP ? 0 : Sh::MINB>;
 	if constexpr (Cfg::SMEM > kMaxSmemPerBlock)
 		return set_error(B200_ERR_UNSUPPORTED, "stencil shape %d needs %d bytes of shared memory",
 				SHAPE, Cfg::SMEM);
