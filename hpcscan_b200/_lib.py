@@ -105,6 +105,7 @@ SIGNATURES = {
     "b200_batch_info": [_VP, ctypes.POINTER(_I)],
     "b200_set_autotune": [_I],
     "b200_get_autotune": [ctypes.POINTER(_I)],
+    "b200_prepare_stencil": [_PL, _I, _I, _I, _I],
     "b200_get_tuned_config": [_PL, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I),
                               ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "b200_set_arith_mode": [_I],

@@ -485,3 +485,64 @@ int autotune_key(const b200_layout* lay, int order, int dtype, int op, int reps,
 
 }  // namespace
 }  // namespace b200
+
+using namespace b200;
+
+extern "C" {
+
+int b200_prepare_stencil(const b200_layout* lay, int order, int dtype, int op, int coef_dtype)
+{
+	if (int rc = check_layout(lay)) return rc;
+	if (int rc = check_order(order)) return rc;
+	if (lay->halo != order / 2) return set_error(B200_ERR_ARG, "layout halo does not match order");
+	if (dtype_size(dtype) == 0) return set_error(B200_ERR_ARG, "dtype %d", dtype);
+	if (op < MODE_D2_AXIS1 || op > MODE_STEP) return set_error(B200_ERR_ARG, "operator %d", op);
+	if (coef_dtype < 0) coef_dtype = dtype;
+	if (dtype_size(coef_dtype) == 0) return set_error(B200_ERR_ARG, "coef dtype %d", coef_dtype);
+	const int64_t inner = (int64_t)(lay->e1 - lay->s1 + 1) * (lay->e2 - lay->s2 + 1) *
+	                      (lay->e3 - lay->s3 + 1);
+	const bool exact = !has_shapes(op) || g_arith == B200_ARITH_EXACT;
+	if (has_shapes(op) && zmarch_accepts(lay, dtype) && autotune_enabled() &&
+			inner >= kAutotuneMinPoints && coef_dtype == dtype) {
+		bool have = false;
+		tuned_for(dtype, order / 2, op, exact, lay, &have);
+		if (!have) {
+			// tuning launches every candidate kernel of the key, which loads them; a grid whose
+			// scratch copies do not fit keeps the defaults (as on first use)
+			std::lock_guard<std::mutex> guard(g_autotune_mutex);
+			const int rc = autotune_key(lay, order, dtype, op, 5);
+			if (rc == B200_ERR_NOMEM) {
+				std::lock_guard<std::mutex> lock(g_tune_mutex);
+				g_tuned[key_of(dtype, order / 2, op, exact, lay)] = default_tuning(dtype, order / 2);
+				return B200_OK;
+			}
+			return rc;
+		}
+		return B200_OK;
+	}
+	// one launch of the operator on zeroed scratch grids of the layout (loads its kernels)
+	const size_t n = (size_t)npoint(lay);
+	void* buf[3] = {nullptr, nullptr, nullptr};
+	const size_t sz[3] = {n * dtype_size(dtype), n * dtype_size(dtype), n * dtype_size(coef_dtype)};
+	int rc = B200_OK;
+	for (int i = 0; i < 3 && !rc; i++) {
+		rc = cuda_error(cudaMalloc(&buf[i], sz[i]), "cudaMalloc(prepare)");
+		if (!rc) rc = cuda_error(cudaMemset(buf[i], 0, sz[i]), "cudaMemset(prepare)");
+	}
+	if (!rc) {
+		const b200_field u{buf[0], dtype, 1.0f}, w{buf[1], dtype, 1.0f}, c{buf[2], coef_dtype, 1.0f};
+		const bool p = op == MODE_PRESSURE || op == MODE_STEP;
+		if (op == MODE_STEP) {
+			rc = b200_propagate_step(lay, order, w, u, c, 1.0, 1.0, 1.0, B200_BOUND_COND_ANTI_MIRROR,
+					nullptr);
+		} else {
+			rc = run_stencil(op, lay, order, u, w, p ? &c : nullptr, 1.0, 1.0, 1.0, nullptr);
+		}
+		if (!rc) rc = cuda_error(cudaDeviceSynchronize(), "cudaDeviceSynchronize(prepare)");
+	}
+	for (void* b : buf)
+		if (b) cudaFree(b);
+	return rc;
+}
+
+}  // extern "C"

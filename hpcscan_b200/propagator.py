@@ -10,6 +10,7 @@ errTestCase = sum1 / sum2 with the reference's FP32 accumulators.
 """
 from __future__ import annotations
 
+import ctypes
 import time
 from dataclasses import dataclass, field
 from typing import Callable, Optional
@@ -65,7 +66,18 @@ class Propagator_Ac2:
         t_prn, t_prc = init_times(s, lay.prec if lay.prec == "f64" else "f32")
         self.initializeGrid(self.prnGrid, t_prn)
         self.initializeGrid(self.prcGrid, t_prc)
+        self.prepare()
         return 0
+
+    def prepare(self) -> None:
+        """Ready the step's kernels before the time loop (b200_prepare_stencil: the first-use
+        tuning for this grid size, or one launch on scratch grids)."""
+        lay = self.prnGrid.c_layout()
+        _lib.call("b200_prepare_stencil", ctypes.byref(lay), self.fdOrder,
+                  _lib.DTYPE_CODE[self.layout.prec], self.prepare_op,
+                  _lib.DTYPE_CODE[self.coef_prec])
+
+    prepare_op = _lib.OP_STEP
 
     def initializeGrid(self, grid: Grid, time_sec) -> int:
         """Eigen mode at time t on ALL_POINTS (src/propagator_Ac2.cpp:441-545)."""
@@ -108,6 +120,7 @@ class Propagator_Ac2SplitComp(Propagator_Ac2):
     """Laplacian then updatePressure (src/propagator_Ac2SplitComp.cpp:72-85)."""
 
     kernel_type = "With Laplacian operator"
+    prepare_op = _lib.OP_LAPLACIAN
 
     def initialize(self, **kw) -> int:
         rc = super().initialize(**kw)

@@ -331,6 +331,13 @@ int b200_autotune_stencil(const b200_layout* lay, int order, int dtype, int op, 
 int b200_set_autotune(int mode);
 int b200_get_autotune(int* mode);
 
+/* Readies the kernels of (layout, order, dtype, op) before a timed loop: the first-use tuning
+ * where it applies, else one launch of the operator on zeroed scratch grids of the layout
+ * (allocated, synchronised and freed here), so that the loop's first call pays neither the
+ * tuning nor the loading of its kernels. coef_dtype: the coef grid's storage (-1: dtype).
+ * Synchronous. No reference counterpart. */
+int b200_prepare_stencil(const b200_layout* lay, int order, int dtype, int op, int coef_dtype);
+
 /* The launch parameters a grid of this layout gets for (dtype, order, op): tile shape, planes
  * per CTA (0 = heuristic), fused step chosen (op 6), and whether they come from a measurement
  * or an explicit setting (*measured = 1) or from the defaults (0). No device work. */
