@@ -207,16 +207,27 @@ class Grid:
     def FD_LAPLACIAN(self, pType: int, W: "Grid", fdOrder: int, stream=None) -> int:
         return self._fd(0, W, fdOrder, "FD_LAPLACIAN", stream)
 
+    def _same_geometry(self, caller: str, *grids: "Grid") -> bool:
+        """Every grid a kernel reads with this grid's layout must have its array geometry (the
+        library indexes them all with one layout); a grid of another geometry is refused here,
+        before any launch (its array would be read past its end)."""
+        for g in grids:
+            if not self.sameSize(g):
+                print_error(f"In Grid::{caller}, grids have not same size")
+                return False
+        return True
+
     def updatePressure(self, pType: int, prc: "Grid", coef: "Grid", lapla: "Grid",
                        stream=None) -> int:
+        if not self._same_geometry("updatePressure", prc, coef, lapla):
+            return RTN_CODE_KO
         lay = self.c_layout()
         _lib.call("b200_update_pressure", ctypes.byref(lay), self.c_field(), prc.c_field(),
                   coef.c_field(), lapla.c_field(), _stream_ptr(stream))
         return RTN_CODE_OK
 
     def computePressureWithFD(self, prc: "Grid", coef: "Grid", fdOrder: int, stream=None) -> int:
-        if not self.sameSize(prc):
-            print_error("In Grid::computePressureWithFD, grids have not same size")
+        if not self._same_geometry("computePressureWithFD", prc, coef):
             return RTN_CODE_KO
         i1, i2, i3 = self.inv2()
         lay = self.c_layout()
@@ -228,8 +239,7 @@ class Grid:
                       boundCondType: int = _lib.B200_BOUND_COND_ANTI_MIRROR, stream=None) -> int:
         """prc.applyBoundaryCondition(boundCondType) then self.computePressureWithFD(prc, coef)
         in one library call (b200_propagate_step)."""
-        if not self.sameSize(prc):
-            print_error("In Grid::computePressureWithFD, grids have not same size")
+        if not self._same_geometry("computePressureWithFD", prc, coef):
             return RTN_CODE_KO
         i1, i2, i3 = self.inv2()
         lay = self.c_layout()

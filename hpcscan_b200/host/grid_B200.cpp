@@ -506,7 +506,8 @@ Rtn_code Grid_B200::propagateStep(Grid& prcGridIn, Grid& coefGridIn, Myint fdOrd
 	printDebug(FULL_DEBUG, "In Grid_B200::propagateStep");
 	Grid_B200* prc = dynamic_cast<Grid_B200*>(&prcGridIn);
 	const Grid_B200* coef = peer(coefGridIn, "Grid_B200::propagateStep");
-	if (!prc || !coef || this->sameSize(prcGridIn) != true || prc->bc_pending != 0x3F || dim != DIM3)
+	if (!prc || !coef || this->sameSize(prcGridIn) != true || this->sameSize(coefGridIn) != true ||
+			prc->bc_pending != 0x3F || dim != DIM3)
 		return computePressureWithFD(prcGridIn, coefGridIn, fdOrder);
 	// every face of a single-rank 3-D grid: the library's step (the fused kernel where the
 	// tuner measured it faster, else the boundary-condition and pressure kernels)
@@ -614,6 +615,11 @@ Rtn_code Grid_B200::updatePressure(Point_type, const Grid& prcGrid, const Grid& 
 	const Grid_B200* coef = peer(coefGrid, "Grid_B200::updatePressure");
 	const Grid_B200* lapla = peer(laplaGrid, "Grid_B200::updatePressure");
 	if (!prc || !coef || !lapla) return RTN_CODE_KO;
+	// the library reads every grid with this grid's layout
+	if (!sameSize(prcGrid) || !sameSize(coefGrid) || !sameSize(laplaGrid)) {
+		printError("In Grid::updatePressure, grids have not same size");
+		return RTN_CODE_KO;
+	}
 	host_ahead = false;
 	if (!ok(b200_update_pressure(&lay, field(), prc->field(), coef->field(), lapla->field(), nullptr),
 				"Grid_B200::updatePressure"))
@@ -631,6 +637,10 @@ Rtn_code Grid_B200::computePressureWithFD(Grid& prcGridIn, Grid& coefGridIn, Myi
 	const Grid_B200* prc = peer(prcGridIn, "Grid_B200::computePressureWithFD");
 	const Grid_B200* coef = peer(coefGridIn, "Grid_B200::computePressureWithFD");
 	if (!prc || !coef) return RTN_CODE_KO;
+	if (this->sameSize(coefGridIn) != true) {        // read with this grid's layout
+		printError("In Grid::computePressureWithFD, grids have not same size");
+		return RTN_CODE_KO;
+	}
 	host_ahead = false;
 	Myfloat64 i2[3];
 	inv2(i2);

@@ -75,3 +75,18 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(_lib.B200Error):
         _lib.load()
+
+
+def test_pressure_refuses_grids_of_another_geometry():
+    """A coef grid laid out for another storage type (here FP32 padding against FP16
+    wavefields, a different n1) is refused on the host before any library call: the kernels
+    read every grid with the wavefield's layout, so its array would be read past its end."""
+    from hpcscan_b200 import layout as L
+    from hpcscan_b200.grid import Grid, RTN_CODE_KO
+    lay16 = L.b200_layout(3, 64, 40, 30, order=8, prec="f16")
+    lay32 = L.b200_layout(3, 64, 40, 30, order=8, prec="f32")
+    assert lay16.n1 != lay32.n1
+    prn, prc, coef = Grid(lay16), Grid(lay16), Grid(lay32)     # no device arrays: never reached
+    assert prn.computePressureWithFD(prc, coef, 8) == RTN_CODE_KO
+    assert prn.propagateStep(prc, coef, 8) == RTN_CODE_KO
+    assert prn.updatePressure(L.INNER_POINTS, prc, coef, prc) == RTN_CODE_KO
