@@ -107,8 +107,6 @@ __global__ void __launch_bounds__(256) k_survey_gradient(const MShot* __restrict
 			const int i1 = a.x0 + 4 * xv, i2 = a.s2 + y, i3 = a.s3 + z;
 			const int64_t idx = (int64_t)i3 * a.n12 + (int64_t)i2 * a.n1 + i1;
 			float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-			// several shots' loads in flight at once (the sum stays in shot order)
-#pragma unroll 4
 			for (int s = 0; s < ns; s++) {
 				const MShot& m = sh[s];
 				const float g23 = m.g2[i2] * m.g3[i3];
