@@ -71,13 +71,14 @@ def parse_args():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--workload", default="propa",
                    choices=["propa", "adjoint", "modeling", "mixed", "fd", "fdsweep", "dropin",
-                            "sustained"],
+                            "launches", "sustained"],
                    help="propa (default, the headline), adjoint (batched checkpointed gradients), "
                         "modeling (batched uneven forward shots), mixed (16-bit wavefields), "
                         "fd (the FD_D1 / FD_D2 operator test cases), fdsweep (the FD_D2 test "
                         "case over orders, cubes and precisions), dropin (hpcscan's own Propa "
-                        "driver on -testMode B200) or sustained (the headline step back to back "
-                        "for --nt steps, with clocks and power per bin)")
+                        "driver on -testMode B200), launches (one launch of each hot kernel, for "
+                        "a profiler) or sustained (the headline step back to back for --nt "
+                        "steps, with clocks and power per bin)")
     p.add_argument("--shots", type=int, default=0, help="shots (adjoint: 16, modeling: 64)")
     p.add_argument("--nt", type=int, default=0, help="time steps (adjoint: 2000, modeling: 1500)")
     p.add_argument("--checkpoint", type=int, default=45, help="adjoint checkpoint interval")
@@ -1148,6 +1149,71 @@ def fdsweep_arm(a):
     print(json.dumps(line))
 
 
+def launches_arm(a):
+    """One launch of each hot kernel at n^3 (default 512), for a profiler: the pressure update
+    in FP32 at each of --orders (default 8,12), the Laplacian at each of them, and the pressure
+    update on FP16 wavefields (FP32 coef) at the first order; inputs filled on the device (the
+    eigen-mode fields, the test case's sine product). Run with HPCSCAN_B200_AUTOTUNE=0 the
+    launches use the untuned defaults and nothing else of the library runs between them. Prints
+    the device time of each launch (CUDA events) in one JSON line."""
+    import torch
+
+    from hpcscan_b200 import layout as L
+    from hpcscan_b200.grid import Grid, init_device
+
+    init_device(0)
+    n = a.size
+    orders = [int(o) for o in (a.orders.split(",") if a.orders else ["8", "12"])]
+    samp = L.Sampling((1.0 / (n - 1),) * 3, (0.0,) * 3)
+
+    def grid(lay, scale=1.0):
+        g = Grid(lay, samp, scale=scale)
+        g.initializeGrid()
+        return g
+
+    def timed_once(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return round(e0.elapsed_time(e1) * 1e3, 1)
+
+    out = []
+
+    def pressure(order, prec, coef, scale):
+        lay = L.b200_layout(3, n, n, n, order=order, prec=prec)
+        clay = lay if coef == prec else L.GridLayout(dim=3, order=order, prec=coef, a1=lay.a1,
+                                                     a2=lay.a2, a3=lay.a3, n_inner=lay.n_inner)
+        prn, prc, cf = grid(lay, scale), grid(lay, scale), grid(clay)
+        prc.fill(L.ALL_POINTS, L.FUNC_SINE, L.FUNC_SINE, L.FUNC_SINE, L.PI, L.PI, L.PI, 0.5)
+        prn.fill(L.ALL_POINTS, L.FUNC_SINE, L.FUNC_SINE, L.FUNC_SINE, L.PI, L.PI, L.PI, 0.49)
+        cf.fill(L.INNER_POINTS, 2.0e-6)
+        us = timed_once(lambda: prn.computePressureWithFD(prc, cf, order))
+        out.append({"kernel": "computePressureWithFD", "order": order, "wave": prec, "coef": coef,
+                    "us": us})
+
+    def laplacian(order):
+        lay = L.b200_layout(3, n, n, n, order=order, prec="f32")
+        U, W = grid(lay), grid(lay)
+        U.fill(L.ALL_POINTS, L.FUNC_SINE, L.FUNC_SINE, L.FUNC_SINE, L.PI * 4, L.PI * 6, L.PI * 8, 1.0)
+        us = timed_once(lambda: U.FD_LAPLACIAN(L.INNER_POINTS, W, order))
+        out.append({"kernel": "FD_LAPLACIAN", "order": order, "wave": "f32", "us": us})
+
+    for o in orders:
+        pressure(o, "f32", "f32", 1.0)
+    for o in orders:
+        laplacian(o)
+    pressure(orders[0], "f16", "f32", 16.0)
+    st = ctypes_status()
+    if st:
+        raise RuntimeError(f"device-side error word {st}")
+    print(json.dumps({"workload": f"one launch per hot kernel, {n}^3", "launches": out,
+                      "note": "single cold launches for a profiler; bench figures come from the "
+                              "other workloads"}))
+
+
 def dropin_arm(a):
     """hpcscan's own Propa test case, unchanged, on -testMode B200 (hpcscan_b200/host/bin): its
     'Best Gpoint/s in FD' (inner points x steps / the propagator's compute-pressure timer, a host
@@ -1314,7 +1380,7 @@ def main():
         if world > 1 and rank != 0:
             return
         {"mixed": mixed_arm, "fd": fd_arm, "fdsweep": fdsweep_arm, "dropin": dropin_arm,
-         "sustained": sustained_arm}[a.workload](a)
+         "launches": launches_arm, "sustained": sustained_arm}[a.workload](a)
         return
     if a.impl == "reference":
         reference_arm(a)
