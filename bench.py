@@ -873,10 +873,8 @@ def modeling_arm(a):
                      "frac": round(16 * pts / t_batched / 1e9 / peak_job, 4),
                      "peak_source": peak_src + (f" x {world} GPUs" if world > 1 else "")},
         "seconds": round(t_batched, 3),
-        "batched_form": "all shots in every launch, the whole gradient in one CUDA graph, CTAs of "
-                        "one tile of every shot side by side, the survey gradient accumulated "
-                        "over the shots in one stencil-free pass per step (timed, with the final "
-                        "all-reduce under torchrun)",
+        "batched_form": "all shots in every launch (a CTA range per shot), the time loop in one "
+                        "CUDA graph",
     }
     if plain is not None:
         t_plain, same = plain
