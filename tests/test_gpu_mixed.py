@@ -59,3 +59,34 @@ def test_16bit_wavefields_against_fp64_oracle(gpu, prec, coef_prec, scale, tol):
     # the reference's analytic check stays within its own threshold (src/testCase_Propa.cpp:91)
     print(f"{prec}/{coef_prec} errTestCase {res.err_test_case:.4e} (FP64 oracle {err64:.4e})")
     assert res.err_test_case < 2e-2
+
+
+def _last_inner_field(torch, prec, coef_prec, scale, n, order, nt):
+    """nt steps of the eigen-mode Propa test (boundary condition + pressure update per step) on
+    the GPU; the last wavefield's inner points as physical FP64 values on the device."""
+    from hpcscan_b200.propagator import Propagator_Ac2
+    lay = L.b200_layout(3, n, n, n, order=order, prec=prec)
+    p = Propagator_Ac2(lay, coef_prec=coef_prec, wave_scale=scale)
+    p.initialize(ratio_cfl=0.8, nt=nt, snap_inc=nt, modes=(1, 1, 1))
+    prn, prc = p.prnGrid, p.prcGrid
+    for _ in range(nt):
+        p.computeWavefieldNextTimeStep(prn, prc)
+        prn, prc = prc, prn
+    out = lay.inner(prc.data.detach()).to(torch.float64) * prc.scale
+    del p, prn, prc
+    torch.cuda.empty_cache()
+    return out
+
+
+def test_fp16_wavefields_512_cubed_1000_steps_within_one_percent_of_fp64(gpu):
+    """The mixed-precision configuration's 512^3 O8 case at its stated length: FP16 wavefields
+    (scale 2^4) with FP32 coef and FP32 arithmetic stay within 1 % (relative L2 of the last
+    wavefield) of the FP64 run of the same 1000 steps, which is itself bit-identical to the
+    reference's FP64 build."""
+    torch = gpu
+    ref = _last_inner_field(torch, "f64", "f64", 1.0, 512, 8, 1000)
+    got = _last_inner_field(torch, "f16", "f32", 2.0 ** 4, 512, 8, 1000)
+    rel = float(torch.linalg.vector_norm((got - ref).flatten()) /
+                torch.linalg.vector_norm(ref.flatten()))
+    print(f"FP16 512^3 O8, 1000 steps: relative L2 to FP64 {rel:.3e}")
+    assert rel < 1e-2, rel
