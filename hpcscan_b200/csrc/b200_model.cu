@@ -76,12 +76,9 @@ constexpr int kRecThreads = 128;
 // Survey gradient of shots on one grid, one step, no stencil: the forward recursion gives
 // C Lap p[n] = (p[n+1] - G amp s[n] delta_src + G^2 p[n-1]) / G - 2 p[n], so
 //   grad += kscale sum_s w_s[n+1] (p_s[n+1] / G_s + G_s p_s[n-1] - 2 p_s[n] - amp_s s[n] delta_src)
-// with the shots summed in batch order. A block takes 16 vectors of four i1 points (rows start
-// 16-byte aligned; the vector of the first inner point may begin in the halo, whose lanes get no
-// contribution and are written back unchanged) and 16 shots at a time, one (shot, vector) per
-// thread, so the loads of 16 shots are in flight together; the threads of shot lane 0 then add
-// the shots' terms in shot order and update the gradient. The shots' pointers are staged in
-// shared memory.
+// with the shots summed in batch order. One thread per 16-byte vector of four i1 points of a
+// row (rows start 16-byte aligned; the vector of the first inner point may begin in the halo,
+// whose lanes are read and written back unchanged), the shots' pointers staged in shared memory.
 struct SurveyArgs {
 	int64_t n1, n12, field;
 	int x0, nvx;                // first vector's i1 (multiple of 4), vectors per row
@@ -91,88 +88,53 @@ struct SurveyArgs {
 	float* grad;
 };
 constexpr int kSurveyMaxShots = 64;      // shots staged per pass over the table
-constexpr int kSurveyLanes = 16;         // shots per step of a block
-constexpr int kSurveyVecs = 16;          // point vectors per block
-constexpr int kSurveyThreads = kSurveyLanes * kSurveyVecs;
 
-__global__ void __launch_bounds__(kSurveyThreads) k_survey_gradient(const MShot* __restrict__ shots,
-		SurveyArgs a)
+__global__ void __launch_bounds__(256) k_survey_gradient(const MShot* __restrict__ shots, SurveyArgs a)
 {
 	__shared__ MShot sh[kSurveyMaxShots];
-	__shared__ float4 sw[kSurveyLanes][kSurveyVecs];     // w of (shot, vector)
-	__shared__ float4 sc[kSurveyLanes][kSurveyVecs];     // C Lap p of (shot, vector)
-	const int lane = threadIdx.x / kSurveyVecs, pv = threadIdx.x % kSurveyVecs;
 	const int ny = a.e2 - a.s2 + 1, nz = a.e3 - a.s3 + 1;
 	const int64_t items = (int64_t)ny * nz * a.nvx;
-	const int64_t groups = (items + kSurveyVecs - 1) / kSurveyVecs;
+	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
 	for (int base = 0; base < a.nshot; base += kSurveyMaxShots) {
 		const int ns = min(kSurveyMaxShots, a.nshot - base);
 		__syncthreads();
 		for (int i = threadIdx.x; i < ns; i += blockDim.x) sh[i] = shots[base + i];
 		__syncthreads();
-		for (int64_t g = blockIdx.x; g < groups; g += gridDim.x) {
-			const int64_t t = g * kSurveyVecs + pv;
-			const bool valid = t < items;
-			int i1 = 0, i2 = 0, i3 = 0;
-			int64_t idx = 0;
-			if (valid) {
-				const int64_t row = t / a.nvx;
-				const int xv = (int)(t - row * a.nvx);
-				const int z = (int)(row / ny), y = (int)(row - (int64_t)z * ny);
-				i1 = a.x0 + 4 * xv;
-				i2 = a.s2 + y;
-				i3 = a.s3 + z;
-				idx = (int64_t)i3 * a.n12 + (int64_t)i2 * a.n1 + i1;
-			}
+		for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < items; t += stride) {
+			const int64_t row = t / a.nvx;
+			const int xv = (int)(t - row * a.nvx);
+			const int z = (int)(row / ny), y = (int)(row - (int64_t)z * ny);
+			const int i1 = a.x0 + 4 * xv, i2 = a.s2 + y, i3 = a.s3 + z;
+			const int64_t idx = (int64_t)i3 * a.n12 + (int64_t)i2 * a.n1 + i1;
 			float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-			for (int sub = 0; sub < ns; sub += kSurveyLanes) {
-				const int s = sub + lane;
-				float4 w4 = make_float4(0.f, 0.f, 0.f, 0.f), c4 = w4;
-				if (valid && s < ns) {
-					const MShot& m = sh[s];
-					const float g23 = m.g2[i2] * m.g3[i3];
-					const float4 g1 = *reinterpret_cast<const float4*>(m.g1 + i1);
-					const float4 p1 = *reinterpret_cast<const float4*>(m.wave + a.snext * a.field + idx);
-					const float4 p0 = *reinterpret_cast<const float4*>(m.wave + a.scur * a.field + idx);
-					const float4 pm = *reinterpret_cast<const float4*>(m.wave + a.sprev * a.field + idx);
-					w4 = *reinterpret_cast<const float4*>(m.adj + a.sadj * a.field + idx);
-					const float G[4] = {g1.x * g23, g1.y * g23, g1.z * g23, g1.w * g23};
-					const float P1[4] = {p1.x, p1.y, p1.z, p1.w}, P0[4] = {p0.x, p0.y, p0.z, p0.w};
-					const float PM[4] = {pm.x, pm.y, pm.z, pm.w};
-					float* C = &c4.x;
+			for (int s = 0; s < ns; s++) {
+				const MShot& m = sh[s];
+				const float g23 = m.g2[i2] * m.g3[i3];
+				const float4 g1 = *reinterpret_cast<const float4*>(m.g1 + i1);
+				const float4 p1 = *reinterpret_cast<const float4*>(m.wave + a.snext * a.field + idx);
+				const float4 p0 = *reinterpret_cast<const float4*>(m.wave + a.scur * a.field + idx);
+				const float4 pm = *reinterpret_cast<const float4*>(m.wave + a.sprev * a.field + idx);
+				const float4 w = *reinterpret_cast<const float4*>(m.adj + a.sadj * a.field + idx);
+				const float G[4] = {g1.x * g23, g1.y * g23, g1.z * g23, g1.w * g23};
+				const float P1[4] = {p1.x, p1.y, p1.z, p1.w}, P0[4] = {p0.x, p0.y, p0.z, p0.w};
+				const float PM[4] = {pm.x, pm.y, pm.z, pm.w}, W[4] = {w.x, w.y, w.z, w.w};
+				float* A = &acc.x;
 #pragma unroll
-					for (int e = 0; e < 4; e++) {
-						if (G[e] == 0.0f) continue;            // halo lanes: G = 0, no term
-						float c = fmaf(G[e], PM[e], __fdiv_rn(P1[e], G[e])) - 2.0f * P0[e];
-						if (idx + e == m.src) c -= m.amp * m.wavelet[a.n];
-						C[e] = c;
-					}
+				for (int e = 0; e < 4; e++) {
+					if (G[e] == 0.0f) continue;            // halo lanes: G = 0 there
+					float c = fmaf(G[e], PM[e], __fdiv_rn(P1[e], G[e])) - 2.0f * P0[e];
+					if (idx + e == m.src) c -= m.amp * m.wavelet[a.n];
+					A[e] = fmaf(W[e], c, A[e]);
 				}
-				sw[lane][pv] = w4;
-				sc[lane][pv] = c4;
-				__syncthreads();
-				if (lane == 0 && valid) {
-					const int nl = min(kSurveyLanes, ns - sub);
-					for (int l = 0; l < nl; l++) {
-						const float4 w = sw[l][pv], c = sc[l][pv];
-						acc.x = fmaf(w.x, c.x, acc.x);
-						acc.y = fmaf(w.y, c.y, acc.y);
-						acc.z = fmaf(w.z, c.z, acc.z);
-						acc.w = fmaf(w.w, c.w, acc.w);
-					}
-				}
-				__syncthreads();
 			}
-			if (lane == 0 && valid) {
-				float4* gp = reinterpret_cast<float4*>(a.grad + idx);
-				float4 gv = *gp;
-				float* G4 = &gv.x;
-				const float* A = &acc.x;
+			float4* gp = reinterpret_cast<float4*>(a.grad + idx);
+			float4 g = *gp;
+			float* G4 = &g.x;
+			const float* A = &acc.x;
 #pragma unroll
-				for (int e = 0; e < 4; e++)
-					if (i1 + e >= a.s1 && i1 + e <= a.e1) G4[e] = fmaf(a.kscale, A[e], G4[e]);
-				*gp = gv;
-			}
+			for (int e = 0; e < 4; e++)
+				if (i1 + e >= a.s1 && i1 + e <= a.e1) G4[e] = fmaf(a.kscale, A[e], G4[e]);
+			*gp = g;
 		}
 	}
 }
@@ -522,9 +484,9 @@ int b200_batch_survey_gradient(b200_batch* b, int n, int snext, int scur, int sp
 	if (a.x0 + 4 * a.nvx > l.n1) return set_error(B200_ERR_ARG, "survey gradient: row vectors");
 	const int64_t items = (int64_t)(l.e2 - l.s2 + 1) * (l.e3 - l.s3 + 1) * a.nvx;
 	const int64_t cap = (int64_t)num_sms() * 8;
-	const int64_t want = (items + kSurveyVecs - 1) / kSurveyVecs;
+	const int64_t want = (items + 255) / 256;
 	const int blocks = (int)(want < cap ? want : cap);
-	k_survey_gradient<<<blocks, kSurveyThreads, 0, as_stream(stream)>>>(b->d_m, a);
+	k_survey_gradient<<<blocks, 256, 0, as_stream(stream)>>>(b->d_m, a);
 	return check_launch("k_survey_gradient");
 }
 
