@@ -85,6 +85,10 @@ def parse_args():
     p.add_argument("--sizes", default="", help="fdsweep: cubes, comma-separated (128,256,512,800)")
     p.add_argument("--orders", default="", help="fdsweep: orders, comma-separated (2,4,8,12,16)")
     p.add_argument("--snap", type=int, default=0, help="dropin: steps between analytic checks (50)")
+    p.add_argument("--survey", type=int, default=1,
+                   help="adjoint: 1 = the batch accumulates the survey gradient in one pass per step "
+                        "(b200_batch_survey_gradient), 0 = each shot's gradient by its own stencil "
+                        "pass, summed after")
     a = p.parse_args()
     if a.size is None:
         a.size = 256 if a.workload == "adjoint" else 512
@@ -694,7 +698,7 @@ def adjoint_arm(a):
     # over all shots, survey=True), and the CTAs of one tile of every shot run side by side (the
     # model tiles then come from DRAM once)
     bat = Batch(shots(vel0, dobs), order, dt, nt, f0, gradient=True, checkpoint=a.checkpoint,
-                device=local, survey=True)
+                device=local, survey=bool(a.survey))
     gsum = torch.empty((n, n, n), dtype=torch.float32, device=dev)
     mem_batched = torch.cuda.memory_allocated() / 1e9
     ctas = bat.ctas_per_pass
@@ -746,10 +750,13 @@ def adjoint_arm(a):
     k = a.checkpoint
     nck = (nt + k - 1) // k
     # algorithmic bytes per shot: forward 16 B/pt-step, recompute 16 B (one step per segment
-    # more for the survey pass), adjoint 16 B, survey gradient 16 B + the gradient's read and
-    # write shared by the shots; checkpoint save (8 B/pt written) and restore (8 B read + 8 B
-    # written) per checkpoint
-    alg = pts * ((16 * nt + 16 * nt + 16 * nt + 16 * nt + 24 * nck) * nshot + 8 * nt * world)
+    # more for the survey pass), adjoint 16 B, and either the survey gradient (16 B per shot + the
+    # gradient's read and write shared by the shots) or each shot's gradient pass (20 B);
+    # checkpoint save (8 B/pt written) and restore (8 B read + 8 B written) per checkpoint
+    if a.survey:
+        alg = pts * ((16 * nt + 16 * nt + 16 * nt + 16 * nt + 24 * nck) * nshot + 8 * nt * world)
+    else:
+        alg = pts * (16 * nt + 16 * (nt - nck) + 16 * nt + 20 * nt + 24 * nck) * nshot
     peak, peak_src = measured_peak()
     peak_job = peak * world
     line = {
@@ -771,14 +778,18 @@ def adjoint_arm(a):
                      "peak": peak_job, "unit": "GB/s",
                      "frac": round(alg / t_batched / 1e9 / peak_job, 4),
                      "peak_source": peak_src + (f" x {world} GPUs" if world > 1 else ""),
-                     "alg_bytes": "per shot-step: 16 forward + 16 recompute + 16 adjoint + 16 "
-                                  "survey gradient, plus 8 per step for the gradient grid and "
-                                  "the checkpoint save/restore"},
+                     "alg_bytes": ("per shot-step: 16 forward + 16 recompute + 16 adjoint + 16 "
+                                   "survey gradient, plus 8 per step for the gradient grid and "
+                                   "the checkpoint save/restore") if a.survey else
+                                  ("per shot-step: 16 forward + 16 recompute + 16 adjoint + 20 "
+                                   "gradient, plus the checkpoint save/restore")},
         "seconds": round(t_batched, 3),
         "batched_form": "all shots in every launch, the whole gradient in one CUDA graph, CTAs of "
-                        "one tile of every shot side by side, the survey gradient accumulated "
-                        "over the shots in one stencil-free pass per step (timed, with the final "
-                        "all-reduce under torchrun)",
+                        "one tile of every shot side by side, " +
+                        ("the survey gradient accumulated over the shots in one stencil-free pass "
+                         "per step" if a.survey else
+                         "each shot's gradient by a stencil pass per step, summed after") +
+                        " (timed, with the final all-reduce under torchrun)",
     }
     if plain is not None:
         t_plain, d = plain
