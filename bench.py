@@ -637,6 +637,23 @@ def _timed(fn, reps=1):
     return e0.elapsed_time(e1) / 1e3 / reps
 
 
+def _graph_timed(fn, reps):
+    """Device seconds per call of fn(stream): reps calls captured in one CUDA graph, the replay
+    timed with CUDA events (after one untimed replay)."""
+    import torch
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g, stream=s):
+        for _ in range(reps):
+            fn(s)
+    g.replay()
+    torch.cuda.synchronize()
+    sec = _timed(g.replay)
+    del g
+    return sec / reps
+
+
 def adjoint_arm(a):
     """Batched checkpointed adjoint gradients vs the plain one-shot-per-launch form.
 
@@ -1077,9 +1094,11 @@ def fdsweep_arm(a):
     """The FD_D2 test case's sweep at its stated sizes: FD_D2_N1/N2/N3 and FD_LAPLACIAN of
     u = sin(4 pi x1) sin(6 pi x2) sin(8 pi x3) on the unit cube (src/testCase_FD_D2.cpp:65-74 with
     -param1 4 -param2 6 -param3 8 -param4 1) for orders 2/4/8/12/16, cubes of 128/256/512/800
-    inner points, FP32 and FP64. Per entry: device time per launch (CUDA events, --steps launches
-    after three warm-up launches; at 256^3 and above the pair of grids exceeds L2, at 128^3 it
-    does not and the figure is marked so), GPoint/s, algorithmic GB/s (read u, write w: 8 B/point
+    inner points, FP32 and FP64. Per entry: device time per launch (--steps launches captured in a
+    CUDA graph, the replay timed with CUDA events, after three warm-up launches; at 256^3 and
+    above the pair of grids exceeds L2, at 128^3 it does not and the figure is marked so), the
+    same launches called one by one from Python (us_per_call_eager: at 128^3 the host path of a
+    call is longer than the kernel), GPoint/s, algorithmic GB/s (read u, write w: 8 B/point
     FP32, 16 FP64) and its fraction of the measured copy bandwidth, and the L1 error against the
     analytic derivative as the test case computes it (Grid::L1Err over the inner points, FP64
     sums on the device)."""
@@ -1115,13 +1134,19 @@ def fdsweep_arm(a):
                         W.fill(L.ALL_POINTS, 0.0)
                         for _ in range(3):
                             fn(L.INNER_POINTS, W, order)
-                        sec = _timed(lambda: fn(L.INNER_POINTS, W, order), reps=a.steps)
-                        launches += 3 + a.steps
+                        eager = _timed(lambda: fn(L.INNER_POINTS, W, order), reps=a.steps)
+                        # the same launches captured in a CUDA graph and replayed: the device
+                        # time of the kernels without the host's per-call path (which, for the
+                        # small cubes, is longer than the kernel)
+                        sec = _graph_timed(lambda st: fn(L.INNER_POINTS, W, order, stream=st),
+                                           a.steps)
+                        launches += 3 + 3 * a.steps
                         R.fill(L.ALL_POINTS, L.FUNC_SINE, L.FUNC_SINE, L.FUNC_SINE, a1, a2, a3, amp)
                         err = W.L1Err(L.INNER_POINTS, R)
                         gbs = bpp * pts / sec / 1e9
                         entries.append({"prec": prec, "n": n, "order": order, "op": op,
                                         "us_per_launch": round(sec * 1e6, 2),
+                                        "us_per_call_eager": round(eager * 1e6, 2),
                                         "gpoint_s": round(pts / sec / 1e9, 2),
                                         "alg_gb_s": round(gbs, 1),
                                         "frac_of_peak": round(gbs / peak, 4),
@@ -1137,8 +1162,8 @@ def fdsweep_arm(a):
     head = [e for e in entries if (e["prec"], e["n"], e["order"], e["op"]) ==
             ("f32", 512, 8, "FD_LAPLACIAN")]
     value = head[0]["gpoint_s"] if head else entries[-1]["gpoint_s"]
-    cols = ["prec", "n", "order", "op", "us_per_launch", "gpoint_s", "alg_gb_s", "frac_of_peak",
-            "l1_err_vs_analytic", "pass_1e-3", "in_l2"]
+    cols = ["prec", "n", "order", "op", "us_per_launch", "us_per_call_eager", "gpoint_s",
+            "alg_gb_s", "frac_of_peak", "l1_err_vs_analytic", "pass_1e-3", "in_l2"]
     line = {
         "metric": "FD_D2 sweep GPoint/s (FD_LAPLACIAN O8 FP32 512^3 as the value; every entry in "
                   "`entries`)",
