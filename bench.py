@@ -85,6 +85,8 @@ def parse_args():
     p.add_argument("--sizes", default="", help="fdsweep: cubes, comma-separated (128,256,512,800)")
     p.add_argument("--orders", default="", help="fdsweep: orders, comma-separated (2,4,8,12,16)")
     p.add_argument("--snap", type=int, default=0, help="dropin: steps between analytic checks (50)")
+    p.add_argument("--propagator", default="Ac2Standard",
+                   help="dropin: hpcscan propagator (Ac2Standard, Ac2SplitComp, Ac2Fused)")
     p.add_argument("--survey", type=int, default=1,
                    help="adjoint: 1 = the batch accumulates the survey gradient in one pass per step "
                         "(b200_batch_survey_gradient), 0 = each shot's gradient by its own stencil "
@@ -1259,7 +1261,7 @@ def dropin_arm(a):
     exe = os.path.join(REPO, "hpcscan_b200", "host", "bin", "hpcscan_b200_fp32")
     n, order, nt = a.size, a.order, a.nt or 200
     snap = a.snap or 50
-    args = [exe, "-testCase", "Propa", "-testMode", "B200", "-propagator", "Ac2Standard",
+    args = [exe, "-testCase", "Propa", "-testMode", "B200", "-propagator", a.propagator,
             "-fdOrder", str(order), "-n1", str(n), "-n2", str(n), "-n3", str(n),
             "-ratioCFL", "0.8", "-nt", str(nt), "-snapInc", str(snap), "-ntry", "1"]
     with tempfile.TemporaryDirectory() as d:
