@@ -85,8 +85,9 @@ TuneKey key_of(int dtype, int R, int mode, bool exact, const b200_layout* lay)
 
 // Untuned defaults: the fastest shape of the pressure update measured at 512^3 on B200 for each
 // storage type and half width, interleaved runs (FP32: the two-row 28x64 tiles up to R = 2, the
-// 14x64 tiles with a four-plane prefetch for R = 3..4, the 14x64 tiles at two CTAs per SM for
-// R = 5..7, the 9-warp 16x64 tiles for R = 8;
+// 14x64 tiles with a four-plane prefetch for R = 3..4, 22x64 tiles of 11 warps with a five-plane
+// prefetch for R = 5..6, the 14x64 tiles at two CTAs per SM for R = 7, the 9-warp 16x64 tiles
+// for R = 8;
 // FP64: 28x32 two-row tiles up to R = 2, 14x32 tiles with the four-plane prefetch for R = 3..5,
 // 16x32 9-warp tiles beyond). 16-bit wavefields (pressure update only): 8-byte thread vectors
 // with the z queue in FP32, 14-row tiles and the four-plane prefetch up to R = 4, 28-row
@@ -96,7 +97,7 @@ Tuned default_tuning(int dtype, int R)
 	Tuned t;
 	if (dtype == B200_F64) t.shape = R <= 2 ? 0 : R <= 5 ? 1 : 2;
 	else if (dtype == B200_F16 || dtype == B200_BF16) t.shape = R <= 4 ? 1 : 2;
-	else t.shape = R <= 2 ? 0 : R <= 4 ? 1 : R <= 7 ? 0 : 2;
+	else t.shape = R <= 2 ? 0 : R <= 4 ? 1 : R <= 6 ? 2 : R == 7 ? 0 : 2;
 	t.nz_chunk = 0;
 	return t;
 }
