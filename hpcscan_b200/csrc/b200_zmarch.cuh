@@ -1008,12 +1008,13 @@ template <typename S, int R> struct Shape<S, R, 0> {
 	                     MINB = (sizeof(S) == 4 && R >= 5 && R <= 7) ? 2 : 0; };
 template <typename S, int R> struct Shape<S, R, 1> {   // shape 0 with a deeper prefetch ring
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 4, MINB = 0; };
-// Shape 2: 9 warps, two CTAs per SM for R <= 4; for FP32 R = 5..6, 11 consumer warps in 22-row
-// tiles at one CTA per SM (up to 168 registers, no spills) with a five-plane prefetch: at 512^3
-// on B200 the pressure update takes 0.478 against 0.523 ms at O10 and 0.488 against 0.566 at O12,
-// the O12 Laplacian 0.45 against 0.51 ms, bit-identical.
+// Shape 2: 9 warps, two CTAs per SM for R <= 4; for FP32 and FP64 R = 5..6, 11 consumer warps in
+// 22-row tiles at one CTA per SM (up to 168 registers, no spills) with a five-plane prefetch: at
+// 512^3 on B200 the FP32 pressure update takes 0.478 against 0.523 ms at O10 and 0.488 against
+// 0.566 at O12, the O12 Laplacian 0.45 against 0.51 ms; FP64 O10 0.93 against 1.13 ms, O12 0.93
+// against 1.15-1.22, the O12 Laplacian 0.92 against 1.03; all bit-identical.
 template <typename S, int R> struct Shape<S, R, 2> {
-	static constexpr bool WIDE = sizeof(S) == 4 && R >= 5 && R <= 6;
+	static constexpr bool WIDE = sizeof(S) >= 4 && R >= 5 && R <= 6;
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = WIDE ? 22 : 16, VY = 1, PF = WIDE ? 5 : 2,
 	                     MINB = (R <= 4 && !WIDE) ? 2 : 1; };
 
