@@ -19,8 +19,11 @@
 // MODE_STEP fuses applyBoundaryCondition(prc, ANTI_MIRROR) into the pressure update: every
 // value the stencils read is the value after the boundary condition, built from the raw
 // tile (halos from mirror points in the same tile, boundary lines and planes as zero, z-halo
-// planes loaded from their mirror planes). The kernel never writes prc, so every CTA reads
-// the raw values; the boundary planes' zeros are written by a separate launch afterwards.
+// planes loaded from their mirror planes). In a CTA whose planes need it, the producer warp
+// rebuilds each plane in shared memory between the copy's arrival and the consumers' release,
+// so the consumers run the pressure update's code unchanged. The kernel never writes prc, so
+// every CTA reads the raw values; the boundary planes' zeros are written by a separate launch
+// afterwards.
 // Every wait on an mbarrier is bounded by a time limit: a CTA that gives up records an
 // error flag (read by b200_device_status) and returns after its issued copies have landed.
 //
@@ -81,10 +84,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 	return ok != 0;
 }
 
-// CTA-local named barrier over `nthreads` threads (a multiple of 32).
-__device__ __forceinline__ void named_barrier_sync(int id, int nthreads)
+// Non-blocking: has the mbarrier phase of the given parity completed?
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity)
 {
-	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+	uint32_t ok;
+	asm volatile(
+			"{\n\t.reg .pred p;\n\t"
+			"mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+			"selp.u32 %0, 1, 0, p;\n\t}"
+			: "=r"(ok)
+			: "r"(smem_u32(bar)), "r"(parity)
+			: "memory");
+	return ok != 0;
+}
+
+// Orders this thread's earlier generic writes to shared memory before later accesses of the
+// same bytes by the async proxy (the TMA copies that refill a slot).
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 __device__ __forceinline__ uint64_t global_timer_ns()
@@ -267,11 +285,12 @@ struct ZCfg {
 	static constexpr int RY = YH ? R : 0;
 	static constexpr int RZ = ZQ ? R : 0;
 	// planes per pass of the z loop (0: four, except two where four would spill registers: the
-	// fused step, the modelling passes, and the pressure update outside R = 3..6; four measured
+	// modelling passes, and the pressure update and fused step outside R = 3..6; four measured
 	// 1.3 % faster than two for the pressure update at 512^3 O8 on B200)
 	static constexpr int UQ = !ZQ ? 1 : UQ_ > 0 ? UQ_
-	                        : (MODE == MODE_STEP || MODE == MODE_MODEL || MODE == MODE_GRAD ||
-	                           (MODE == MODE_PRESSURE && (R < 3 || R > 6))) ? 2 : 4;
+	                        : (MODE == MODE_MODEL || MODE == MODE_GRAD ||
+	                           ((MODE == MODE_PRESSURE || MODE == MODE_STEP) && (R < 3 || R > 6)))
+	                                  ? 2 : 4;
 	static constexpr int BX = TX + 2 * R4;
 	static constexpr int BY = TY + 2 * RY;
 	static constexpr int NSU = (ZONLY && 2 * PF + 4 > RZ + 1 + PF) ? 2 * PF + 4
@@ -290,8 +309,13 @@ struct ZCfg {
 	static constexpr int NC = NTX * (TY / VY);              // consumer threads
 	static constexpr int NWC = NC / 32;                      // consumer warps
 	static constexpr int NT = NC + 32;                       // + one producer warp
+	// fused boundary condition: the producer's patch lists (phase 1: halo points from mirror
+	// points, at most R columns and R rows on each side of the tile; phase 2: boundary lines)
+	static constexpr int NL1 = BC ? 2 * R * BY + 2 * R * BX : 0;
+	static constexpr int NL2 = BC ? 2 * BY + 2 * BX : 0;
+	static_assert(!BC || (PF >= 2 && BX * BY < 0xFFFF), "fused step: patch lag and 16-bit offsets");
 	static constexpr int SMEM = 128 + NSU * U_STRIDE + (P ? NSP * SLOT_P : 0) +
-	                            (2 * NSU + NSP) * 8;
+	                            (2 * NSU + NSP) * 8 + (BC ? NSU * 8 + (NL1 + NL2) * 4 : 0);
 	// CTAs per SM the launch bounds ask for (registers follow: an SM has four sub-partitions
 	// of 16K registers and spreads a CTA's warps over them). Two CTAs per SM for R <= 4 with
 	// 8-warp CTAs; wider stencils keep their longer z queue in registers at one CTA per SM.
@@ -342,6 +366,218 @@ struct Ring {
 	}
 };
 
+// The producer warp of a fused-step CTA whose planes need the boundary condition. Lane 0 issues
+// the copies as the plain producer does, except that they land on land_u; the warp rebuilds
+// each landed plane in its slot (the values applyBoundaryCondition(ANTI_MIRROR) leaves in prc,
+// faces in the reference's order I1, I2, I3: src/grid.cpp:3065-3229) and releases it to the
+// consumers on full_u (lane 0 arrives once the warp's writes are done). One loop does both:
+// copies are issued as soon as their slots are free (the plain producer's depth) and planes
+// are released as soon as they land, so neither waits behind the other.
+template <class Cfg, bool SLOTS>
+__device__ __forceinline__ void step_patch_producer(const CUtensorMap* tm_u,
+		const CUtensorMap* tm_p0, const CUtensorMap* tm_p1, const ZArgs<typename Cfg::C>& a,
+		typename Cfg::Stor* su, unsigned char* sp, uint64_t* bars, int tile_x0, int tile_y0, int z0,
+		int J, bool near, int slot_u, int slot_p0, uint64_t deadline)
+{
+	using S = typename Cfg::Stor;
+	using C = typename Cfg::C;
+	static_assert(Cfg::NPT == 2, "fused step: prn and coef tiles");
+	constexpr int R = Cfg::R, R4 = Cfg::R4, RY = Cfg::RY, RZ = Cfg::RZ, TX = Cfg::TX;
+	constexpr int BX = Cfg::BX, BY = Cfg::BY, NSU = Cfg::NSU, NSP = Cfg::NSP;
+	constexpr int UE = Cfg::U_STRIDE / (int)sizeof(S);
+	constexpr unsigned FULL = 0xffffffffu;
+	constexpr uint32_t NEG_ZERO = 0xFFFFu;     // phase-1 source that stands for a zeroed point
+	uint64_t* full_u = bars;
+	uint64_t* empty_u = bars + NSU;
+	uint64_t* empty_p = bars + 2 * NSU;
+	uint64_t* land_u = bars + 2 * NSU + NSP;
+	uint32_t* list1 = reinterpret_cast<uint32_t*>(bars + 3 * NSU + NSP);
+	uint32_t* list2 = list1 + Cfg::NL1;
+	const int lane = threadIdx.x & 31;
+	const int xs = tile_x0 - R4, xe = tile_x0 + TX + R4 - 1;
+	const int ys = tile_y0 - RY, ye = tile_y0 + Cfg::TY + RY - 1;
+	if (lane == 0) {
+		prefetch_tmap(tm_u);
+		prefetch_tmap(tm_p0);
+		prefetch_tmap(tm_p1);
+	}
+
+	// the tile's patch lists, the same for every inner plane: phase 1 writes halo points from
+	// their mirror points ((dst << 16) | src; src NEG_ZERO writes -0), phase 2 zeroes the points
+	// of the boundary lines
+	int n1 = 0, n2 = 0;
+	if (near) {
+		for (int base = 0; base < Cfg::NL1; base += 32) {
+			const int idx = base + lane;
+			uint32_t e = 0;
+			bool use = false;
+			if (idx < 2 * R * BY) {
+				// i1 halos: -(mirror), before any face zeroes a line
+				const int side = idx / (R * BY), rem = idx % (R * BY);
+				const int kk = rem / BY + 1, r = rem % BY;
+				const int y = ys + r;
+				const int ch = (side ? a.e1 + kk : a.s1 - kk) - xs;
+				const int cm = (side ? a.e1 - kk : a.s1 + kk) - xs;
+				use = y >= a.s2 && y <= a.e2 && ch >= 0 && ch < BX && cm >= 0 && cm < BX;
+				e = (uint32_t)(r * BX + ch) << 16 | (uint32_t)(r * BX + cm);
+			} else if (idx < Cfg::NL1) {
+				// i2 halos: -(mirror), after the i1 faces zeroed their boundary columns
+				const int i2 = idx - 2 * R * BY;
+				const int side = i2 / (R * BX), rem = i2 % (R * BX);
+				const int kk = rem / BX + 1, c = rem % BX;
+				const int x = xs + c;
+				const int rh = (side ? a.e2 + kk : a.s2 - kk) - ys;
+				const int rm = (side ? a.e2 - kk : a.s2 + kk) - ys;
+				use = x >= a.s1 && x <= a.e1 && rh >= 0 && rh < BY && rm >= 0 && rm < BY;
+				e = (uint32_t)(rh * BX + c) << 16 |
+				    ((x == a.s1 || x == a.e1) ? NEG_ZERO : (uint32_t)(rm * BX + c));
+			}
+			const unsigned m = __ballot_sync(FULL, use);
+			if (use) list1[n1 + __popc(m & ((1u << lane) - 1u))] = e;
+			n1 += __popc(m);
+		}
+		for (int base = 0; base < Cfg::NL2; base += 32) {
+			const int idx = base + lane;
+			uint32_t e = 0;
+			bool use = false;
+			if (idx < 2 * BY) {                        // boundary columns s1, e1
+				const int side = idx / BY, r = idx % BY;
+				const int y = ys + r, c = (side ? a.e1 : a.s1) - xs;
+				use = y >= a.s2 && y <= a.e2 && c >= 0 && c < BX;
+				e = (uint32_t)(r * BX + c);
+			} else if (idx < Cfg::NL2) {               // boundary rows s2, e2
+				const int i2 = idx - 2 * BY;
+				const int side = i2 / BX, c = i2 % BX;
+				const int x = xs + c, r = (side ? a.e2 : a.s2) - ys;
+				use = x >= a.s1 && x <= a.e1 && r >= 0 && r < BY;
+				e = (uint32_t)(r * BX + c);
+			}
+			const unsigned m = __ballot_sync(FULL, use);
+			if (use) list2[n2 + __popc(m & ((1u << lane) - 1u))] = e;
+			n2 += __popc(m);
+		}
+		__syncwarp();
+	}
+	// the inner points of the tile with its halos: a rectangle (cw x ch from (cx0, cy0))
+	const int cx0 = max(xs, a.s1) - xs, cy0 = max(ys, a.s2) - ys;
+	const int cw = min(xe, a.e1) - xs - cx0 + 1, ch = min(ye, a.e2) - ys - cy0 + 1;
+	const int ninner = (cw > 0 && ch > 0) ? cw * ch : 0;
+
+	// rebuild plane jj (stream index), landed, in its slot and release it to the consumers
+	auto patch_plane = [&](int jj) {
+		const int slot = jj % NSU;
+		S* tw = su + slot * UE;
+		const int pl = z0 - RZ + jj;
+		bool wrote = false;
+		if (pl < a.s3 || pl > a.e3) {
+			// z-halo plane, loaded from its mirror plane: minus the mirror after the i1/i2 faces
+			// zeroed their lines (only its inner points are read, by the z stencil)
+			for (int r = cy0; r < cy0 + ch; ++r) {
+				const int y = ys + r;
+				const bool yline = y == a.s2 || y == a.e2;
+				for (int c = cx0 + lane; c < cx0 + cw; c += 32) {
+					const int x = xs + c;
+					S& v = tw[r * BX + c];
+					v = Storage<S>::store((yline || x == a.s1 || x == a.e1) ? -C(0) : -Storage<S>::load(v));
+				}
+			}
+			wrote = ninner > 0;
+		} else {
+			for (int i = lane; i < n1; i += 32) {
+				const uint32_t pe = list1[i];
+				const uint32_t src = pe & 0xFFFFu;
+				const C mv = src == NEG_ZERO ? C(0) : Storage<S>::load(tw[src]);
+				tw[pe >> 16] = Storage<S>::store(-mv);
+			}
+			__syncwarp();                          // every mirror point read before lines are zeroed
+			if (pl == a.s3 || pl == a.e3) {
+				// boundary plane: every inner point is zero
+				for (int r = cy0; r < cy0 + ch; ++r)
+					for (int c = cx0 + lane; c < cx0 + cw; c += 32) tw[r * BX + c] = S(0.0f);
+				wrote = true;
+			} else {
+				for (int i = lane; i < n2; i += 32) tw[list2[i]] = S(0.0f);
+				wrote = n1 > 0 || n2 > 0;
+			}
+		}
+		// the patch's writes before the slot is refilled by a copy (the async proxy), and before
+		// lane 0's release of the plane (the warp barrier orders them before its arrival)
+		if (wrote) fence_proxy_async_smem();
+		__syncwarp();
+		if (lane == 0) mbar_arrive(&full_u[slot]);
+	};
+
+	bool ok = true;
+	int issued = 0, patched = 0;
+	Ring<NSU> wu;
+	Ring<NSP> wp;
+	while (patched < J) {
+		// every copy whose slots are free (the consumers released their previous use)
+		while (issued < J) {
+			const int j = issued;
+			const bool pw = j >= 2 * RZ;
+			bool go = true;
+			if (lane == 0) {
+				go = (j < NSU || mbar_test(&empty_u[wu.slot], wu.phase ^ 1u)) &&
+				     (!pw || j - 2 * RZ < NSP || mbar_test(&empty_p[wp.slot], wp.phase ^ 1u));
+				if (go) {
+					int plane = z0 - RZ + j;           // z-halo planes come from their mirrors
+					if (plane < a.s3) plane = 2 * a.s3 - plane;
+					else if (plane > a.e3) plane = 2 * a.e3 - plane;
+					uint64_t* bar = &land_u[wu.slot];
+					mbar_arrive_expect_tx(bar, Cfg::U_BYTES + (pw ? Cfg::SLOT_TX : 0));
+					tma_tile<SLOTS>(su + wu.slot * UE, tm_u, xs, ys, plane, slot_u, bar);
+					if (pw) {
+						const int o = j - 2 * RZ;
+						unsigned char* slot = sp + wp.slot * Cfg::SLOT_P;
+						tma_tile<SLOTS>(slot, tm_p0, tile_x0, tile_y0, z0 + o, slot_p0, bar);
+						tma_tile<SLOTS>(slot + Cfg::PT_STRIDE, tm_p1, tile_x0, tile_y0, z0 + o, 0, bar);
+					}
+				}
+			}
+			if (!__shfl_sync(FULL, go, 0)) break;
+			++issued;
+			wu.advance();
+			if (pw) wp.advance();
+		}
+		// every issued plane that has landed, oldest first
+		while (patched < issued) {
+			const uint32_t par = (uint32_t)(patched / NSU) & 1u;
+			bool landed = false;
+			if (lane == 0) landed = mbar_test(&land_u[patched % NSU], par);
+			if (!__shfl_sync(FULL, landed, 0)) break;
+			(void)mbar_test(&land_u[patched % NSU], par);   // every lane acquires the copy's bytes
+			patch_plane(patched);
+			++patched;
+		}
+		if (patched == J) break;
+		// nothing to do: sleep in the barrier unit until the oldest copy lands or, with every
+		// issued plane released, until the next slot is free (each wait bounded by the hardware's
+		// own time limit; the loop then checks again)
+		if (lane == 0) {
+			if (patched < issued) {
+				(void)mbar_try_wait(&land_u[patched % NSU], (uint32_t)(patched / NSU) & 1u);
+			} else if (issued >= NSU && !mbar_test(&empty_u[wu.slot], wu.phase ^ 1u)) {
+				(void)mbar_try_wait(&empty_u[wu.slot], wu.phase ^ 1u);
+			} else {
+				(void)mbar_try_wait(&empty_p[wp.slot], wp.phase ^ 1u);   // the pointwise slot
+			}
+			if (global_timer_ns() > deadline) ok = false;
+		}
+		if (!__shfl_sync(FULL, ok, 0)) {
+			ok = false;
+			break;
+		}
+	}
+	if (!ok && lane == 0) atomicOr(a.err, 1u);
+	// every issued copy lands before the CTA may retire its shared memory (the patched ones did)
+	if (lane == 0) {
+		const uint64_t drain = global_timer_ns() + a.timeout_ns;
+		for (int jj = max(patched, issued - NSU); jj < issued; ++jj)
+			mbar_wait(&land_u[jj % NSU], (uint32_t)(jj / NSU) & 1u, drain);
+	}
+}
+
 // The kernel body: one CTA, tile (bx, by) of (i1, i2), z-chunk bz. tm_p[0..NPT) are the
 // pointwise tiles of the output plane. SLOTS: the grids are slotted (4-D tensor maps whose
 // outermost coordinate is the slot), as the modelling engine keeps its wavefields.
@@ -359,7 +595,6 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	constexpr int R4 = Cfg::R4, RY = Cfg::RY, RZ = Cfg::RZ, BX = Cfg::BX;
 	constexpr int NSU = Cfg::NSU, NSP = Cfg::NSP, NC = Cfg::NC;
 	constexpr int UE = Cfg::U_STRIDE / (int)sizeof(S);     // elements between input tiles
-	constexpr unsigned FULL = 0xffffffffu;
 
 	extern __shared__ unsigned char smem_raw[];
 	unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -372,6 +607,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	uint64_t* full_u = bars;
 	uint64_t* empty_u = bars + NSU;
 	uint64_t* empty_p = bars + 2 * NSU;      // the pointwise tiles land on full_u (see the producer)
+	uint64_t* land_u = bars + 2 * NSU + NSP; // fused step: where the copies land before the patch
 
 	const int tile_x0 = a.x_start + bx * TX;
 	const int tile_y0 = a.s2 + by * Cfg::TY;
@@ -379,10 +615,24 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	const int z1 = min(z0 + a.nz_chunk, a.e3 + 1);
 	const int J = (z1 - z0) + 2 * RZ;          // planes this CTA streams in
 
+	// fused boundary condition: a CTA whose tile (with halos) comes within R of an i1 or i2
+	// boundary line, or whose planes include a boundary or z-halo plane, has its planes rebuilt
+	// by the producer warp; the others run the pressure update as it is
+	bool near = false, patch = false;
+	if constexpr (Cfg::BC) {
+		const int xs = tile_x0 - R4, xe = tile_x0 + TX + R4 - 1;
+		const int ys = tile_y0 - RY, ye = tile_y0 + Cfg::TY + RY - 1;
+		near = (xs <= a.s1 + R && xe >= a.s1 - R) || (xs <= a.e1 + R && xe >= a.e1 - R) ||
+		       (ys <= a.s2 + R && ye >= a.s2 - R) || (ys <= a.e2 + R && ye >= a.e2 - R);
+		patch = near || z0 - RZ <= a.s3 || z1 - 1 + RZ >= a.e3;
+	}
+
 	if (threadIdx.x == 0) {
 		for (int s = 0; s < NSU; s++) {
+			// one arrival completes a plane: the copy's (expect_tx), or the patching warp's lane 0
 			mbar_init(&full_u[s], 1);
 			mbar_init(&empty_u[s], NC);        // every consumer thread releases
+			if constexpr (Cfg::BC) mbar_init(&land_u[s], 1);
 		}
 		for (int s = 0; s < NSP; s++) {
 			mbar_init(&empty_p[s], NC);
@@ -393,6 +643,13 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	const uint64_t deadline = global_timer_ns() + a.timeout_ns;
 
 	if (threadIdx.x >= NC) {
+		if constexpr (Cfg::BC) {
+			if (patch) {
+				step_patch_producer<Cfg, SLOTS>(tm_u, tm_p0, tm_p1, a, su, sp, bars, tile_x0, tile_y0,
+						z0, J, near, slot_u, slot_p0, deadline);
+				return;
+			}
+		}
 		// ---- producer: one thread issues every TMA copy ------------------------------------------
 		if (threadIdx.x != NC) return;
 		prefetch_tmap(tm_u);
@@ -418,12 +675,7 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 				ok = false;
 				break;
 			}
-			int plane = z0 - RZ + j;
-			if constexpr (Cfg::BC) {
-				// z-halo planes are rebuilt from their mirror planes by the consumers
-				if (plane < a.s3) plane = 2 * a.s3 - plane;
-				else if (plane > a.e3) plane = 2 * a.e3 - plane;
-			}
+			const int plane = z0 - RZ + j;     // (a fused step's z-halo planes: patching producer)
 			uint64_t* bar = &full_u[wu.slot];
 			mbar_arrive_expect_tx(bar, Cfg::U_BYTES + (pw ? Cfg::SLOT_TX : 0));
 			tma_tile<SLOTS>(su + wu.slot * UE, tm_u, tile_x0 - R4, tile_y0 - RY, plane, slot_u, bar);
@@ -480,77 +732,6 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 	rc.slot = RZ;                      // stage RZ: first centre plane (RZ < NSU, use 0)
 	Ring<NSP> rp;                      // prn/coef of output plane j - 2 RZ
 
-	// ---- fused boundary condition: per-thread constants, the same for every plane ----
-	// A CTA whose tile (with halos) comes within R of an i1 or i2 boundary line rebuilds, in
-	// shared memory, the values the boundary condition leaves: phase 1 writes the halo points
-	// from their mirror points (i1 halos = -(mirror) before any face; i2 halos = -(mirror)
-	// after the i1 faces zeroed their boundary columns), phase 2 zeroes the boundary lines and,
-	// on a boundary plane, every inner point (reference face order I1, I2, I3). Each thread
-	// owns a fixed list of tile offsets for both phases.
-	constexpr int BYc = Cfg::BY;
-	constexpr int NP1 = Cfg::BC ? (2 * R * BYc + 2 * R * BX + NC - 1) / NC : 1;
-	constexpr int NP2 = Cfg::BC ? (2 * BYc + 2 * BX + NC - 1) / NC : 1;
-	constexpr uint32_t NO_PATCH = 0xFFFFFFFFu, NEG_ZERO = 0xFFFFu;
-	bool near = false;
-	uint32_t p1[NP1];                  // phase 1: (dst << 16) | src, src NEG_ZERO writes -0
-	uint32_t p2[NP2];                  // phase 2: offset to zero
-	uint32_t qline = 0;                // bits over the thread's points that lie on a boundary line
-	if constexpr (Cfg::BC) {
-		const int xs = tile_x0 - R4, xe = tile_x0 + TX + R4 - 1;
-		const int ys = tile_y0 - RY, ye = tile_y0 + Cfg::TY + RY - 1;
-		near = (xs <= a.s1 + R && xe >= a.s1 - R) || (xs <= a.e1 + R && xe >= a.e1 - R) ||
-		       (ys <= a.s2 + R && ye >= a.s2 - R) || (ys <= a.e2 + R && ye >= a.e2 - R);
-#pragma unroll
-		for (int v = 0; v < VY; v++)
-#pragma unroll
-			for (int e = 0; e < VX; e++) {
-				const int x = X + e, y = Y0 + v;
-				if (x == a.s1 || x == a.e1 || y == a.s2 || y == a.e2) qline |= 1u << (v * VX + e);
-			}
-		const int nxband = 2 * R * BYc, nyband = 2 * R * BX;
-#pragma unroll
-		for (int m = 0; m < NP1; m++) {
-			p1[m] = NO_PATCH;
-			const int idx = tid + m * NC;
-			if (!near) continue;
-			if (idx < nxband) {
-				const int side = idx / (R * BYc), rem = idx % (R * BYc);
-				const int kk = rem / BYc + 1, r = rem % BYc;
-				const int y = ys + r;
-				const int ch = (side ? a.e1 + kk : a.s1 - kk) - xs;
-				const int cm = (side ? a.e1 - kk : a.s1 + kk) - xs;
-				if (y >= a.s2 && y <= a.e2 && ch >= 0 && ch < BX && cm >= 0 && cm < BX)
-					p1[m] = (uint32_t)(r * BX + ch) << 16 | (uint32_t)(r * BX + cm);
-			} else if (idx < nxband + nyband) {
-				const int i2 = idx - nxband;
-				const int side = i2 / (R * BX), rem = i2 % (R * BX);
-				const int kk = rem / BX + 1, c = rem % BX;
-				const int x = xs + c;
-				const int rh = (side ? a.e2 + kk : a.s2 - kk) - ys;
-				const int rm = (side ? a.e2 - kk : a.s2 + kk) - ys;
-				if (x >= a.s1 && x <= a.e1 && rh >= 0 && rh < BYc && rm >= 0 && rm < BYc)
-					p1[m] = (uint32_t)(rh * BX + c) << 16 |
-					        ((x == a.s1 || x == a.e1) ? NEG_ZERO : (uint32_t)(rm * BX + c));
-			}
-		}
-#pragma unroll
-		for (int m = 0; m < NP2; m++) {
-			p2[m] = NO_PATCH;
-			const int idx = tid + m * NC;
-			if (!near) continue;
-			if (idx < 2 * BYc) {                       // boundary columns s1, e1
-				const int side = idx / BYc, r = idx % BYc;
-				const int y = ys + r, c = (side ? a.e1 : a.s1) - xs;
-				if (y >= a.s2 && y <= a.e2 && c >= 0 && c < BX) p2[m] = (uint32_t)(r * BX + c);
-			} else if (idx < 2 * BYc + 2 * BX) {       // boundary rows s2, e2
-				const int i2 = idx - 2 * BYc;
-				const int side = i2 / BX, c = i2 % BX;
-				const int x = xs + c, r = (side ? a.e2 : a.s2) - ys;
-				if (x >= a.s1 && x <= a.e1 && r >= 0 && r < BYc) p2[m] = (uint32_t)(r * BX + c);
-			}
-		}
-	}
-
 	// this thread's first point of output plane z0 (advanced by one plane per output plane; the
 	// stores check their bounds)
 	S* orow = static_cast<S*>(a.out) + X + (int64_t)Y0 * a.n1 + (int64_t)z0 * a.n12;
@@ -563,44 +744,21 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 		const int j = jb + u;
 		if (j >= J) return;
 			const int s = ru.slot;
-			if constexpr (Cfg::BC) {
-				// the fused boundary condition's named barriers need the lanes of a warp to agree
-				if (alive && !__all_sync(FULL, mbar_wait(&full_u[s], ru.phase, deadline))) alive = false;
-			} else {
-				// lanes give up on their own (each then skips its work; no barrier follows)
-				if (alive && !mbar_wait(&full_u[s], ru.phase, deadline)) alive = false;
-			}
+			// lanes give up on their own (each then skips its work; no barrier follows)
+			if (alive && !mbar_wait(&full_u[s], ru.phase, deadline)) alive = false;
 			if constexpr (Cfg::ZQ) {
 				if (alive) {
 					const S* t = su + s * UE;
 #pragma unroll
 					for (int v = 0; v < VY; v++)
 						Q::template push<VX>(t + (yl + v + RY) * BX + R4 + xl, q[u + 2 * RZ][v]);
-					if constexpr (Cfg::BC) {
-						// values after the boundary condition: boundary lines and planes are zero; a
-						// z-halo plane (loaded from its mirror) is minus the mirror after the i1/i2
-						// faces zeroed their lines
-						const int plane = z0 - RZ + j;
-						const bool mir = plane < a.s3 || plane > a.e3;
-						const bool zb = plane == a.s3 || plane == a.e3;
-						if (near || mir || zb) {
-#pragma unroll
-							for (int v = 0; v < VY; v++)
-#pragma unroll
-								for (int e = 0; e < VX; e++) {
-									const bool line = (qline >> (v * VX + e)) & 1u;
-									C& val = q[u + 2 * RZ][v][e];
-									if (mir) val = line ? -C(0) : -val;
-									else if (line || zb) val = C(0);
-								}
-						}
-					}
 				}
 			}
 			if constexpr (Cfg::ZONLY) mbar_arrive(&empty_u[s]);
 			if (j >= 2 * RZ) {
 				const int o = j - 2 * RZ;
 				const int k = z0 + o;                     // output plane
+				(void)k;
 				const int sc = Cfg::ZQ ? rc.slot : s;      // slot holding plane k with its halos
 				const S* t = su + sc * UE;
 				const S* pt = nullptr;     // output-plane tile (prn, or w for the gradient)
@@ -613,48 +771,14 @@ __device__ __forceinline__ void zmarch_body(const CUtensorMap* tm_u, const CUten
 					ct = reinterpret_cast<const SC*>(slot + Cfg::PT_STRIDE);
 					gt = reinterpret_cast<const S*>(slot + Cfg::PT_STRIDE + Cfg::CT_STRIDE);
 				}
-				const bool kb = Cfg::BC && (k == a.s3 || k == a.e3);
-				if constexpr (Cfg::BC) {
-					if (near || kb) {
-						S* tw = su + sc * UE;
-						if (alive && near) {
-#pragma unroll
-							for (int m = 0; m < NP1; m++) {
-								const uint32_t pe = p1[m];
-								if (pe == NO_PATCH) continue;
-								const uint32_t src = pe & 0xFFFFu;
-								const C mv = src == NEG_ZERO ? C(0) : Storage<S>::load(tw[src]);
-								tw[pe >> 16] = Storage<S>::store(-mv);
-							}
-						}
-						named_barrier_sync(1, NC);   // every consumer warp, alive or not
-						if (alive) {
-							if (near) {
-#pragma unroll
-								for (int m = 0; m < NP2; m++)
-									if (p2[m] != NO_PATCH) tw[p2[m]] = S(0.0f);
-							}
-							if (kb) {                // boundary plane: every inner point is zero
-								const int xs = tile_x0 - R4, ys = tile_y0 - RY;
-								for (int idx = tid; idx < BX * BYc; idx += NC) {
-									const int r = idx / BX, c = idx - r * BX;
-									const int x = xs + c, y = ys + r;
-									if (x >= a.s1 && x <= a.e1 && y >= a.s2 && y <= a.e2) tw[idx] = S(0.0f);
-								}
-							}
-						}
-						named_barrier_sync(1, NC);
-					}
-				}
 				if (alive) {
-					// rows of this thread's columns, plane k: (VY + 2 RY) x VX values (near a
-					// boundary the centre rows come from the patched tile too: a thread's vector
-					// can straddle the last inner point, and its halo part needs the patch)
+					// rows of this thread's columns, plane k: (VY + 2 RY) x VX values, the centre
+					// rows from the z queue
 					typename Q::T yv[VY + 2 * RY][VQ];
 #pragma unroll
 					for (int r = 0; r < VY + 2 * RY; r++) {
 						const int v = r - RY;
-						if (v >= 0 && v < VY && Cfg::ZQ && !(Cfg::BC && (near || kb))) {
+						if (v >= 0 && v < VY && Cfg::ZQ) {
 #pragma unroll
 							for (int e = 0; e < VQ; e++) yv[r][e] = q[u + RZ][v < 0 ? 0 : (v >= VY ? VY - 1 : v)][e];
 						} else {
@@ -1030,9 +1154,8 @@ int launch_shape(const ZLaunch& L)
 	// registers there): 0.22 against 0.32 ms for FD_D2_N2 O16 FP32 at 512^3 on B200 (at O8 the
 	// one-row tiles are as fast).
 	constexpr bool YROWS = (MODE == MODE_D2_AXIS2 || MODE == MODE_D1_AXIS2) && R >= 5;
-	// the fused step keeps its registers (its in-tile boundary condition spills at 128)
 	using Cfg = ZCfg<S, R, MODE, Sh::TX, YROWS ? 56 : Sh::TY, YROWS ? 4 : Sh::VY, Sh::PF, EXACT,
-			MODE == MODE_STEP ? 0 : Sh::MINB>;
+			Sh::MINB>;
 	if constexpr (Cfg::SMEM > kMaxSmemPerBlock)
 		return set_error(B200_ERR_UNSUPPORTED, "stencil shape %d needs %d bytes of shared memory",
 				SHAPE, Cfg::SMEM);

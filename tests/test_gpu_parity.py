@@ -383,7 +383,10 @@ STEP_LAYOUTS = [L.b200_layout(3, 37, 20, 23, order=8), L.b200_layout(3, 70, 33, 
                 L.b200_layout(3, 21, 22, 20, order=2), L.b200_layout(3, 45, 27, 29, order=6),
                 L.b200_layout(3, 52, 31, 40, order=12, prec="f64"),
                 L.b200_layout(3, 37, 20, 23, order=8, prec="f64"),
-                L.b200_layout(3, 33, 40, 22, order=14), L.b200_layout(3, 29, 21, 25, order=10)]
+                L.b200_layout(3, 33, 40, 22, order=14), L.b200_layout(3, 29, 21, 25, order=10),
+                # tiles and z-chunks clear of every boundary (the fused step's unpatched CTAs)
+                L.b200_layout(3, 200, 60, 50, order=8),
+                L.b200_layout(3, 120, 60, 50, order=12, prec="f64")]
 
 
 def propagate_step(lay, prn, prc, coef, samp):
