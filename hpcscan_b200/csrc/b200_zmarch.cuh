@@ -1127,11 +1127,17 @@ template <typename S, int R, int SHAPE> struct Shape;
 // 170-200 registers these would take otherwise leaves the schedulers short of warps: at 512^3 on
 // B200 the pressure update takes 0.51 against 0.64 ms at O10, 0.58 against 0.66 at O12, 0.59
 // against 0.62 at O14, bit-identical; at O16 the spills make it slower).
+// UQP: planes per pass of the z loop for the pressure update and the fused step (0: the
+// default of the mode).
 template <typename S, int R> struct Shape<S, R, 0> {
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 2,
-	                     MINB = (sizeof(S) == 4 && R >= 5 && R <= 7) ? 2 : 0; };
-template <typename S, int R> struct Shape<S, R, 1> {   // shape 0 with a deeper prefetch ring
-	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 4, MINB = 0; };
+	                     MINB = (sizeof(S) == 4 && R >= 5 && R <= 7) ? 2 : 0, UQP = 0; };
+// shape 0 with a deeper prefetch ring; FP32 R = 4 with eight planes per pass of the pressure
+// update's z loop (half the queue shifts and loop overhead per plane; 128 registers, no spills;
+// 0.349 against 0.355 ms at 512^3 on B200)
+template <typename S, int R> struct Shape<S, R, 1> {
+	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = (R <= 2 ? 28 : 14), VY = (R <= 2 ? 2 : 1), PF = 4, MINB = 0,
+	                     UQP = (sizeof(S) == 4 && R == 4) ? 8 : 0; };
 // Shape 2: 9 warps, two CTAs per SM for R <= 4; for FP32 and FP64 R = 5..6, 11 consumer warps in
 // 22-row tiles at one CTA per SM (up to 168 registers, no spills) with a five-plane prefetch: at
 // 512^3 on B200 the FP32 pressure update takes 0.478 against 0.523 ms at O10 and 0.488 against
@@ -1140,7 +1146,7 @@ template <typename S, int R> struct Shape<S, R, 1> {   // shape 0 with a deeper 
 template <typename S, int R> struct Shape<S, R, 2> {
 	static constexpr bool WIDE = sizeof(S) >= 4 && R >= 5 && R <= 6;
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = WIDE ? 22 : 16, VY = 1, PF = WIDE ? 5 : 2,
-	                     MINB = (R <= 4 && !WIDE) ? 2 : 1; };
+	                     MINB = (R <= 4 && !WIDE) ? 2 : 1, UQP = 0; };
 
 // Shared memory a CTA may use on sm_100 (227 KB).
 constexpr int kMaxSmemPerBlock = 232448;
@@ -1155,7 +1161,7 @@ int launch_shape(const ZLaunch& L)
 	// one-row tiles are as fast).
 	constexpr bool YROWS = (MODE == MODE_D2_AXIS2 || MODE == MODE_D1_AXIS2) && R >= 5;
 	using Cfg = ZCfg<S, R, MODE, Sh::TX, YROWS ? 56 : Sh::TY, YROWS ? 4 : Sh::VY, Sh::PF, EXACT,
-			Sh::MINB>;
+			Sh::MINB, S, (MODE == MODE_PRESSURE || MODE == MODE_STEP) ? Sh::UQP : 0>;
 	if constexpr (Cfg::SMEM > kMaxSmemPerBlock)
 		return set_error(B200_ERR_UNSUPPORTED, "stencil shape %d needs %d bytes of shared memory",
 				SHAPE, Cfg::SMEM);
