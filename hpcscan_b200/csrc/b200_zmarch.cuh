@@ -285,11 +285,11 @@ struct ZCfg {
 	static constexpr int RY = YH ? R : 0;
 	static constexpr int RZ = ZQ ? R : 0;
 	// planes per pass of the z loop (0: four, except two where four would spill registers: the
-	// modelling passes, and the pressure update and fused step outside R = 3..6; four measured
-	// 1.3 % faster than two for the pressure update at 512^3 O8 on B200)
+	// pressure update, fused step and modelling passes outside R = 3..6; four measured 1.3 %
+	// faster than two for the pressure update at 512^3 O8 on B200)
 	static constexpr int UQ = !ZQ ? 1 : UQ_ > 0 ? UQ_
-	                        : (MODE == MODE_MODEL || MODE == MODE_GRAD ||
-	                           ((MODE == MODE_PRESSURE || MODE == MODE_STEP) && (R < 3 || R > 6)))
+	                        : ((MODE == MODE_PRESSURE || MODE == MODE_STEP || MODE == MODE_MODEL ||
+	                            MODE == MODE_GRAD) && (R < 3 || R > 6))
 	                                  ? 2 : 4;
 	static constexpr int BX = TX + 2 * R4;
 	static constexpr int BY = TY + 2 * RY;
