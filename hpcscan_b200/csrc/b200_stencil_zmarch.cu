@@ -97,7 +97,7 @@ Tuned default_tuning(int dtype, int R)
 	Tuned t;
 	if (dtype == B200_F64) t.shape = R <= 2 ? 0 : R <= 4 ? 1 : 2;
 	else if (dtype == B200_F16 || dtype == B200_BF16) t.shape = R <= 4 ? 1 : 2;
-	else t.shape = R <= 2 ? 0 : R <= 4 ? 1 : R <= 6 ? 2 : R == 7 ? 0 : 2;
+	else t.shape = R <= 2 ? 0 : R <= 4 ? 1 : 2;
 	t.nz_chunk = 0;
 	return t;
 }
