@@ -1143,15 +1143,17 @@ template <typename S, int R> struct Shape<S, R, 1> {
 // 512^3 on B200 the FP32 pressure update takes 0.478 against 0.523 ms at O10 and 0.488 against
 // 0.566 at O12, the O12 Laplacian 0.45 against 0.51 ms; FP64 O10 0.93 against 1.13 ms, O12 0.93
 // against 1.15-1.22, the O12 Laplacian 0.92 against 1.03; all bit-identical.
-// FP32 R = 7..8 and FP64 R = 7: the 9-warp tile with a deeper prefetch (four planes for FP32
-// R = 7, five otherwise) and four planes per pass of the pressure update's z loop; at 512^3 on
-// B200: FP32 O16 0.571 against 0.635 ms (the O16 Laplacian 0.51 against 0.55), FP32 O14 0.517
-// against 0.553 on the two-CTA tile of shape 0, FP64 O14 1.12 against 1.25.
+// R = 7..8: the 9-warp tile with a deeper prefetch (four planes for FP32 R = 7 and FP64 R = 8,
+// where five would not leave the fused step's shared memory room, five otherwise) and four
+// planes per pass of the pressure update's z loop; at 512^3 on B200: FP32 O16 0.571 against
+// 0.635 ms (the O16 Laplacian 0.51 against 0.55), FP32 O14 0.517 against 0.553 on the two-CTA
+// tile of shape 0, FP64 O14 1.12 against 1.25, FP64 O16 1.24 against 1.26 (Laplacian 1.13
+// against 1.16).
 template <typename S, int R> struct Shape<S, R, 2> {
 	static constexpr bool WIDE = sizeof(S) >= 4 && R >= 5 && R <= 6;
-	static constexpr bool DEEP = (sizeof(S) == 4 && (R == 7 || R == 8)) || (sizeof(S) == 8 && R == 7);
+	static constexpr bool DEEP = sizeof(S) >= 4 && (R == 7 || R == 8);
 	static constexpr int TX = 64 * 4 / (int)sizeof(S), TY = WIDE ? 22 : 16, VY = 1,
-	                     PF = WIDE ? 5 : DEEP ? ((sizeof(S) == 4 && R == 7) ? 4 : 5) : 2,
+	                     PF = WIDE ? 5 : DEEP ? ((sizeof(S) == 4) == (R == 7) ? 4 : 5) : 2,
 	                     MINB = (R <= 4 && !WIDE) ? 2 : 1, UQP = DEEP ? 4 : 0; };
 
 // Shared memory a CTA may use on sm_100 (227 KB).
