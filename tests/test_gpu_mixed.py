@@ -61,6 +61,36 @@ def test_16bit_wavefields_against_fp64_oracle(gpu, prec, coef_prec, scale, tol):
     assert res.err_test_case < 2e-2
 
 
+@pytest.mark.parametrize("order", [10, 12, 14, 16])
+@pytest.mark.parametrize("prec,scale,tol", [("f16", 2.0 ** 4, 1e-2), ("bf16", 1.0, 4e-2)])
+def test_16bit_wavefields_high_orders_against_fp64_oracle(gpu, order, prec, scale, tol):
+    """The 16-bit pressure kernels of the high orders (22-row tiles at O10-O12, the deeper
+    9-warp tile at O14-O16), FP32 coef: 40 eigen-mode steps within the same bounds of the FP64
+    oracle as at O8."""
+    from hpcscan_b200.propa_setup import eigen_setup
+    from hpcscan_b200.propagator import run_propa
+    from oracle import oracle
+    n, nt, snap = (72, 56, 48), 40, 20
+    lay = L.b200_layout(3, *n, order=order, prec=prec)
+    assert route(lay) == 1
+    got = {}
+    run_propa(lay, ratio_cfl=0.8, nt=nt, snap_inc=snap, modes=(1, 1, 1), coef_prec="f32",
+              wave_scale=scale,
+              on_check=lambda it, prn, ref: got.__setitem__(it, lay.inner(prn.to_numpy()).astype(np.float64)))
+    # the FP64 oracle on the same array geometry (the grid origin follows the layout's first
+    # inner index, which the 16-bit and FP64 layouts place differently at some orders)
+    import dataclasses
+    lay64 = dataclasses.replace(lay, prec="f64")
+    setup = eigen_setup(lay, ratio_cfl=0.8, nt=nt, snap_inc=snap, modes=(1, 1, 1))
+    want = {}
+    oracle.propagate(lay64, setup, on_check=lambda it, prn, ref: want.__setitem__(it, lay64.inner(prn).copy()))
+    peak = max(np.linalg.norm(w) for w in want.values())
+    for it in want:
+        e = np.linalg.norm(got[it] - want[it]) / peak
+        print(f"{prec} O{order} step {it}: relative L2 error vs FP64 oracle {e:.3e}")
+        assert e < tol, (it, e)
+
+
 def _last_inner_field(torch, prec, coef_prec, scale, n, order, nt):
     """nt steps of the eigen-mode Propa test (boundary condition + pressure update per step) on
     the GPU; the last wavefield's inner points as physical FP64 values on the device."""
